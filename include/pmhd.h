@@ -1,0 +1,169 @@
+/*
+ * pmhd.h -- C ABI of libpmhd.so, the B200 (sm_100a) 2D ideal-MHD + mixed-GLM
+ * finite-volume solver.
+ *
+ * The reference exposes this path only as a command-line program and a
+ * header-only point interface; it has no library API.  Each entry point
+ * below replaces one piece of the reference's host driver
+ * src/mhd/mhd2d_glm_gpu.cu (paths are inside the reference project):
+ *
+ *   pmhd_config_default / pmhd_create   argv parsing + cudaMalloc of the
+ *                                       state arrays (mhd2d_glm_gpu.cu:353-472)
+ *   pmhd_init_problem                   host initial conditions + H2D copy
+ *                                       + first applyBC (:414-474)
+ *   pmhd_set_state / pmhd_get_state     the H2D / D2H state copies (:473, :546)
+ *   pmhd_advance                        the time loop while (t < t_end)
+ *                                       (:482-537): CFL reduction, two SSPRK2
+ *                                       stages, positivity checks
+ *   pmhd_get_stats                      step count, t, c_h(last) and the HLLD
+ *                                       fallback counters printed at :548-589
+ *   pmhd_diagnostics                    divB / psi norms (:556-574)
+ *   pmhd_write_dat                      the .dat output file (:591-648)
+ *   pmhd_destroy                        the cudaFree calls (:650-651)
+ *   pmhd_strerror                       the stderr messages of the exit codes
+ *
+ * Conventions
+ *   - Every function returns an int status: PMHD_OK (0) or a pmhd_status
+ *     code.  Codes 1..9 mirror the reference program's exit codes; the
+ *     library never calls exit().
+ *   - State buffers passed in or out are HOST memory owned by the caller, in
+ *     the reference's array-of-structures order: conserved variables
+ *     (rho, rho*vx, rho*vy, rho*vz, E, Bx, By, Bz, psi) innermost, then i,
+ *     then j.  Element type: double for PMHD_FP64 and PMHD_MIXED, float for
+ *     PMHD_FP32.  Device memory is owned by the handle.
+ *   - A handle is used by one host thread at a time and runs on its own CUDA
+ *     stream; distinct handles are independent.
+ */
+#ifndef PMHD_H
+#define PMHD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMHD_ABI_VERSION 1
+
+typedef enum {
+  PMHD_OK = 0,
+  PMHD_ERR_ARG = 1,          /* invalid argument (reference exit code 1)        */
+  PMHD_ERR_RATE = 2,         /* non-positive maximum signal rate (exit code 2)  */
+  PMHD_ERR_STAGE1 = 3,       /* non-physical state after RK stage 1 (code 3)    */
+  PMHD_ERR_STAGE2 = 4,       /* non-physical state after RK stage 2 (code 4)    */
+  PMHD_ERR_IO = 5,           /* cannot open the output file (code 5)            */
+  PMHD_ERR_CUDA = 9,         /* CUDA runtime error (code 9)                     */
+  PMHD_ERR_TIMEOUT = -1,     /* a bounded device-side wait expired              */
+  PMHD_ERR_NOMEM = -2,       /* device allocation failed                        */
+  PMHD_ERR_UNSUPPORTED = -3, /* configuration not supported by this build       */
+  PMHD_ERR_NODEVICE = -4     /* no CUDA device of compute capability 10.0       */
+} pmhd_status;
+
+typedef enum { PMHD_FP64 = 0, PMHD_FP32 = 1, PMHD_MIXED = 2 } pmhd_precision;
+typedef enum { PMHD_BC_PERIODIC = 0, PMHD_BC_REFLECT = 1, PMHD_BC_TRANSMISSIVE = 2 } pmhd_bc;
+typedef enum { PMHD_ORDER_FIRST = 0, PMHD_ORDER_MUSCL = 1 } pmhd_order;
+typedef enum { PMHD_SOLVER_HLL = 0, PMHD_SOLVER_HLLD = 1 } pmhd_solver_kind;
+typedef enum {
+  PMHD_PROBLEM_ORSZAG_TANG = 0, /* mhd2d_glm_gpu.cu:443-451, unit periodic box        */
+  PMHD_PROBLEM_KH_REF = 1,      /* the reference's doubly periodic double shear layer */
+  PMHD_PROBLEM_KH_REFLECT = 2,  /* single shear layer, x periodic, y reflecting       */
+  PMHD_PROBLEM_BRIO_WU_2D = 3   /* Brio-Wu Riemann problem, interface rotated         */
+} pmhd_problem;
+typedef enum { PMHD_LAYOUT_INTERIOR = 0, PMHD_LAYOUT_GHOSTED = 1 } pmhd_layout;
+
+typedef struct {
+  int nx, ny;                       /* interior cells                          */
+  double x_min, x_max, y_min, y_max;
+  double gamma;                     /* ratio of specific heats                 */
+  double hlld_tol;                  /* HLLD relative degeneracy tolerance      */
+  double cfl;                       /* CFL number, 0 < cfl < 1                 */
+  double alpha;                     /* GLM damping parameter, rate = c_h/alpha */
+  int order;                        /* pmhd_order (MUSCL + SSPRK2 or first)    */
+  int solver;                       /* pmhd_solver_kind                        */
+  int precision;                    /* pmhd_precision                          */
+  int exact;                        /* 1: kernels built without FMA contraction
+                                       (bit-parity mode), 0: FMA enabled      */
+  int bc[4];                        /* x low, x high, y low, y high (pmhd_bc)  */
+  int device;                       /* CUDA device ordinal                     */
+  int steps_per_graph;              /* steps captured per CUDA graph, 0 = auto */
+} pmhd_config;
+
+typedef struct {
+  long long steps;                  /* steps taken since creation / set_state */
+  double t;                         /* current simulation time                */
+  double ch_last;                   /* c_h of the last step taken             */
+  double dt_last;                   /* dt of the last step taken              */
+  unsigned long long x_evals;       /* HLLD flux evaluations, x interfaces    */
+  unsigned long long y_evals;       /* HLLD flux evaluations, y interfaces    */
+  unsigned long long degenerate;    /* HLLD -> HLL fallbacks, degenerate      */
+  unsigned long long nonphysical;   /* HLLD -> HLL fallbacks, non-physical    */
+  int status;                       /* status of the last advance             */
+  int bad_i, bad_j;                 /* first unusable cell (status 3 or 4)    */
+  long long bad_step;               /* step index of that failure             */
+  unsigned long long kernel_launches; /* kernels that did work, total        */
+  double device_ms;                 /* GPU time of the last pmhd_advance, from
+                                       CUDA events on the handle's stream     */
+} pmhd_stats;
+
+typedef struct pmhd_solver pmhd_solver;
+
+/* Fills the reference CLI defaults: 128 x 128 on [0,1]^2, gamma 5/3, HLLD
+ * tolerance 1e-4, CFL 0.25, alpha 0.18, MUSCL, HLLD, fp64, FMA, periodic. */
+int pmhd_config_default(pmhd_config* cfg);
+
+/* Allocates the device state for cfg on cfg->device.  *out is NULL on error. */
+int pmhd_create(const pmhd_config* cfg, pmhd_solver** out);
+
+int pmhd_destroy(pmhd_solver* s);
+
+/* Builds problem `problem` on the host and uploads it; resets t and the
+ * step count to 0.  params may be NULL (defaults) or point to:
+ *   ORSZAG_TANG:   params[0] = field amplitude factor B0 (1 = reference)
+ *   KH_REFLECT:    params[0] = shear-layer width (0.05), params[1] = Bx (0.1)
+ *   BRIO_WU_2D:    params[0] = interface angle in radians (0)
+ * gamma, domain and boundary kinds are taken from the handle's config. */
+int pmhd_init_problem(pmhd_solver* s, int problem, const double* params, int nparams);
+
+/* Copies a host state into the solver and resets t and the step count.
+ * layout INTERIOR: ny*nx*9 values; GHOSTED: (ny+4)*(nx+4)*9 values (the
+ * reference's array; ghost values are rebuilt from the boundary kinds). */
+int pmhd_set_state(pmhd_solver* s, const void* host, int layout);
+
+/* Copies the current state to host memory (layout as for set_state; the
+ * GHOSTED form includes the ghost values the solver holds). */
+int pmhd_get_state(pmhd_solver* s, void* host, int layout);
+
+/* Sets the simulation time and step count (e.g. after set_state of a
+ * restart). */
+int pmhd_set_time(pmhd_solver* s, double t, long long steps);
+
+/* Advances while t < t_end and fewer than max_steps steps were taken in this
+ * call (max_steps < 0: no step limit).  Returns PMHD_OK, or PMHD_ERR_STAGE1 /
+ * PMHD_ERR_STAGE2 with stats->bad_i/bad_j/bad_step set.  stats may be NULL. */
+int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* stats);
+
+int pmhd_get_stats(const pmhd_solver* s, pmhd_stats* stats);
+
+/* divB L1, divB Linf and psi Linf of the current state, computed on the host
+ * exactly as the reference does (central differences, mhd2d_glm_gpu.cu:556-574). */
+int pmhd_diagnostics(pmhd_solver* s, double out[3]);
+
+/* Writes the reference .dat file (header lines + one data line per cell:
+ * x y rho vx vy vz p Bx By Bz E divB psi).  title: first header line without
+ * the leading "# "; order/solver/precision names go into the second line. */
+int pmhd_write_dat(pmhd_solver* s, const char* path, const char* title);
+
+/* Output file name the reference would use for this configuration:
+ * {prob}_glm_{order}_{solver}_{fp64|fp32|mixed}_N{nx}x{ny}.dat */
+int pmhd_dat_filename(const pmhd_solver* s, const char* prob_base, char* buf, size_t len);
+
+const char* pmhd_strerror(int status);
+
+/* Copies the configuration a handle was created with. */
+int pmhd_get_config(const pmhd_solver* s, pmhd_config* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMHD_H */

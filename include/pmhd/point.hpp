@@ -1,0 +1,474 @@
+// pmhd/point.hpp -- header-only per-point ideal-MHD + mixed-GLM numerics,
+// compiled both as host code (g++) and as device code (nvcc, sm_100a).
+//
+// This is the B200 build's replacement for the reference's header-only
+// Real/HD layer (include/base.hpp, include/mhd/mhd_common.hpp,
+// include/mhd/mhd_glm_common.hpp).  Differences in form, not in arithmetic:
+//   * every function is a template on the arithmetic type T, so one source
+//     serves the binary64, binary32 and mixed-precision kernels;
+//   * gamma and the HLLD tolerance are runtime values (Phys<T>) so batched
+//     runs can mix gamma = 5/3 and gamma = 2 in one launch;
+//   * the normal direction is a template parameter AX (0 = x, 1 = y).  The
+//     reference solves y-faces by permuting the state into x order, calling
+//     the x routine and permuting back (mhd_common.hpp:381-405, :658-667);
+//     here the routine reads the permuted slots directly, which performs the
+//     same operations on the same values.
+// Each expression keeps the reference's association order, so with
+// contraction disabled (-fmad=false on device, -ffp-contract=off on host)
+// the binary64 results are bit-identical to the reference CPU build.
+//
+// The reference-named compatibility API (mhdHlldFluxX, mhdGlmFluxY, ...)
+// lives in pmhd/compat/mhd/mhd_glm_common.hpp on top of this file.
+#ifndef PMHD_POINT_HPP
+#define PMHD_POINT_HPP
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define PMHD_HD __host__ __device__ __forceinline__
+#else
+#define PMHD_HD inline
+#endif
+
+namespace pmhd {
+
+// Conserved slots (reference MHDIndex + MHD_GLM_PSI, mhd_common.hpp:81-90,
+// mhd_glm_common.hpp:26-27).  Primitive slots reuse 1..4 for vx, vy, vz, p.
+enum Slot : int { RHO = 0, MX = 1, MY = 2, MZ = 3, EN = 4, BX = 5, BY = 6, BZ = 7, PSI = 8 };
+constexpr int NV8 = 8;
+constexpr int NV9 = 9;
+
+// HLLD status codes (mhd_common.hpp:438-440).
+enum HlldStatus : int { HLLD_OK = 0, HLLD_FALLBACK_DEGENERATE = 1, HLLD_FALLBACK_NONPHYSICAL = 2 };
+
+template <class T>
+struct Phys {
+  T gamma;  // ratio of specific heats
+  T gm1;    // gamma - 1, evaluated as (gamma - 1) in T
+  T tol;    // HLLD relative degeneracy tolerance
+  PMHD_HD static Phys make(double g, double tolerance) {
+    Phys p;
+    p.gamma = (T)g;
+    p.gm1 = p.gamma - (T)1.0;
+    p.tol = (T)tolerance;
+    return p;
+  }
+};
+
+template <class T> PMHD_HD T rho_floor() { return (T)1.0e-12; }
+template <class T> PMHD_HD T p_floor() { return (T)1.0e-12; }
+
+// max/min/abs/sqrt: device uses fmax/fmin (as the reference device path
+// does), host uses the std::max/std::min comparison form.
+template <class T> PMHD_HD T vmax(T a, T b) {
+#ifdef __CUDA_ARCH__
+  return fmax(a, b);
+#else
+  return (a < b) ? b : a;
+#endif
+}
+template <class T> PMHD_HD T vmin(T a, T b) {
+#ifdef __CUDA_ARCH__
+  return fmin(a, b);
+#else
+  return (b < a) ? b : a;
+#endif
+}
+template <class T> PMHD_HD T vabs(T a) {
+#ifdef __CUDA_ARCH__
+  return fabs(a);
+#else
+  return std::fabs(a);
+#endif
+}
+template <class T> PMHD_HD T vsqrt(T a) {
+#ifdef __CUDA_ARCH__
+  return sqrt(a);
+#else
+  return std::sqrt(a);
+#endif
+}
+template <class T> PMHD_HD bool vfinite(T a) {
+#ifdef __CUDA_ARCH__
+  return isfinite((double)a);
+#else
+  return std::isfinite((double)a);
+#endif
+}
+
+// Slot map of a normal direction: n = normal, t1/t2 = tangential.
+template <int AX>
+struct Dir {
+  static constexpr int vn = AX ? MY : MX, vt1 = AX ? MX : MY, vt2 = MZ;
+  static constexpr int bn = AX ? BY : BX, bt1 = AX ? BX : BY, bt2 = BZ;
+};
+
+// Minmod limiter (mhd_common.hpp:140-143).
+template <class T> PMHD_HD T minmod(T a, T b) {
+  if (a * b <= (T)0.0) return (T)0.0;
+  return (vabs(a) < vabs(b)) ? a : b;
+}
+
+// W -> U, 8 slots (mhd_common.hpp:149-173), sums in x, y, z order.
+template <class T>
+PMHD_HD void prim_to_cons(const T* W, T* U, const Phys<T>& ph) {
+  const T rho = W[RHO], vx = W[MX], vy = W[MY], vz = W[MZ], p = W[EN];
+  const T bx = W[BX], by = W[BY], bz = W[BZ];
+  const T v2 = vx * vx + vy * vy + vz * vz;
+  const T b2 = bx * bx + by * by + bz * bz;
+  U[RHO] = rho;
+  U[MX] = rho * vx;
+  U[MY] = rho * vy;
+  U[MZ] = rho * vz;
+  U[EN] = p / ph.gm1 + (T)0.5 * rho * v2 + (T)0.5 * b2;
+  U[BX] = bx;
+  U[BY] = by;
+  U[BZ] = bz;
+}
+
+// U -> W, 8 slots (mhd_common.hpp:178-201).  AX selects the summation order
+// of |v|^2 and |B|^2 (normal, t1, t2), which is what the reference's
+// rotated y-direction calls compute.
+template <class T, int AX = 0>
+PMHD_HD void cons_to_prim(const T* U, T* W, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T rho = vmax(U[RHO], rho_floor<T>());
+  const T vn = U[D::vn] / rho, vt1 = U[D::vt1] / rho, vt2 = U[D::vt2] / rho;
+  const T bn = U[D::bn], bt1 = U[D::bt1], bt2 = U[D::bt2];
+  const T v2 = vn * vn + vt1 * vt1 + vt2 * vt2;
+  const T b2 = bn * bn + bt1 * bt1 + bt2 * bt2;
+  const T p = ph.gm1 * (U[EN] - (T)0.5 * rho * v2 - (T)0.5 * b2);
+  W[RHO] = rho;
+  W[D::vn] = vn;
+  W[D::vt1] = vt1;
+  W[D::vt2] = vt2;
+  W[EN] = p;
+  W[D::bn] = bn;
+  W[D::bt1] = bt1;
+  W[D::bt2] = bt2;
+}
+
+// Fast magnetosonic speed along AX (mhd_common.hpp:206-238).
+template <class T, int AX>
+PMHD_HD T fast_speed(const T* W, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T rho = vmax(W[RHO], rho_floor<T>());
+  const T p = vmax(W[EN], p_floor<T>());
+  const T bn = W[D::bn], bt1 = W[D::bt1], bt2 = W[D::bt2];
+  const T a2 = ph.gamma * p / rho;
+  const T b2 = (bn * bn + bt1 * bt1 + bt2 * bt2) / rho;
+  const T can2 = bn * bn / rho;
+  T disc = (a2 + b2) * (a2 + b2) - (T)4.0 * a2 * can2;
+  disc = vmax(disc, (T)0.0);
+  const T cf2 = (T)0.5 * (a2 + b2 + vsqrt(disc));
+  return vsqrt(vmax(cf2, (T)0.0));
+}
+
+// Physical ideal-MHD flux along AX from primitives W and total energy e
+// (mhdFluxXW / mhdFluxYW, mhd_common.hpp:247-308).
+template <class T, int AX>
+PMHD_HD void phys_flux(const T* W, T e, T* F) {
+  using D = Dir<AX>;
+  const T rho = W[RHO], vn = W[D::vn], vt1 = W[D::vt1], vt2 = W[D::vt2], p = W[EN];
+  const T bn = W[D::bn], bt1 = W[D::bt1], bt2 = W[D::bt2];
+  const T b2 = bn * bn + bt1 * bt1 + bt2 * bt2;
+  const T ptot = p + (T)0.5 * b2;
+  const T vdotb = vn * bn + vt1 * bt1 + vt2 * bt2;
+  F[RHO] = rho * vn;
+  F[D::vn] = rho * vn * vn + ptot - bn * bn;
+  F[D::vt1] = rho * vn * vt1 - bn * bt1;
+  F[D::vt2] = rho * vn * vt2 - bn * bt2;
+  F[EN] = (e + ptot) * vn - bn * vdotb;
+  F[D::bn] = (T)0.0;
+  F[D::bt1] = vn * bt1 - bn * vt1;
+  F[D::bt2] = vn * bt2 - bn * vt2;
+}
+
+// HLL flux along AX (mhdHllFluxX / mhdHllFluxY, mhd_common.hpp:323-377).
+template <class T, int AX>
+PMHD_HD void hll_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  T WL[NV8], WR[NV8], FL[NV8], FR[NV8];
+  cons_to_prim<T, AX>(UL, WL, ph);
+  cons_to_prim<T, AX>(UR, WR, ph);
+  phys_flux<T, AX>(WL, UL[EN], FL);
+  phys_flux<T, AX>(WR, UR[EN], FR);
+  const T cfL = fast_speed<T, AX>(WL, ph);
+  const T cfR = fast_speed<T, AX>(WR, ph);
+  const T sL = vmin(WL[D::vn] - cfL, WR[D::vn] - cfR);
+  const T sR = vmax(WL[D::vn] + cfL, WR[D::vn] + cfR);
+  if (sL >= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FL[k];
+  } else if (sR <= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FR[k];
+  } else {
+    const T denom = sR - sL;
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = (sR * FL[k] - sL * FR[k] + sL * sR * (UR[k] - UL[k])) / denom;
+  }
+}
+
+// Scale-aware smallness test (mhdHlldIsSmall, mhd_common.hpp:417-419).
+template <class T> PMHD_HD bool hlld_small(T v, T scale, const Phys<T>& ph) {
+  return vabs(v) <= ph.tol * scale;
+}
+
+// Positive density and pressure; the negated comparison also rejects NaN
+// (mhdConservedHasPositivePressure, mhd_common.hpp:426-431).
+template <class T, int AX>
+PMHD_HD bool positive_state(const T* U, const Phys<T>& ph) {
+  if (!(U[RHO] > rho_floor<T>())) return false;
+  T W[NV8];
+  cons_to_prim<T, AX>(U, W, ph);
+  return (W[RHO] > rho_floor<T>() && W[EN] > p_floor<T>());
+}
+
+// Star state behind an outer fast wave of speed s (mhdHlldStarStateX,
+// mhd_common.hpp:445-511).  bn is the (shared) normal field.
+template <class T, int AX>
+PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
+                      const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T rho = vmax(W[RHO], rho_floor<T>());
+  const T vn = W[D::vn], vt1 = W[D::vt1], vt2 = W[D::vt2];
+  const T p = vmax(W[EN], p_floor<T>());
+  const T bt1 = W[D::bt1], bt2 = W[D::bt2];
+  const T e = U[EN];
+  const T smv = s - vn;
+  const T sms = s - sm;
+  const T wave_scale = vmax(vabs(s), vabs(sm));
+  if (hlld_small(sms, wave_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
+  const T rho_s = rho * smv / sms;
+  if (rho_s <= rho_floor<T>()) return HLLD_FALLBACK_NONPHYSICAL;
+  const T denom = rho * smv * sms - bn * bn;
+  const T denom_scale = vabs(rho * smv * sms) + bn * bn;
+  if (hlld_small(denom, denom_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
+  const T common = sm - vn;
+  const T vt1_s = vt1 - bn * bt1 * common / denom;
+  const T vt2_s = vt2 - bn * bt2 * common / denom;
+  const T bt1_s = bt1 * (rho * smv * smv - bn * bn) / denom;
+  const T bt2_s = bt2 * (rho * smv * smv - bn * bn) / denom;
+  const T b2 = bn * bn + bt1 * bt1 + bt2 * bt2;
+  const T pt = p + (T)0.5 * b2;
+  const T vdotb = vn * bn + vt1 * bt1 + vt2 * bt2;
+  const T vbs = sm * bn + vt1_s * bt1_s + vt2_s * bt2_s;
+  const T e_s = (smv * e - pt * vn + pt_star * sm + bn * (vdotb - vbs)) / sms;
+  Us[RHO] = rho_s;
+  Us[D::vn] = rho_s * sm;
+  Us[D::vt1] = rho_s * vt1_s;
+  Us[D::vt2] = rho_s * vt2_s;
+  Us[EN] = e_s;
+  Us[D::bn] = bn;
+  Us[D::bt1] = bt1_s;
+  Us[D::bt2] = bt2_s;
+  return positive_state<T, AX>(Us, ph) ? HLLD_OK : HLLD_FALLBACK_NONPHYSICAL;
+}
+
+// HLLD flux along AX (Miyoshi & Kusano 2005 with the reference's
+// scale-aware guards; mhdHlldFluxX, mhd_common.hpp:518-654).  Degenerate or
+// non-physical intermediate states fall back to HLL at this interface and
+// return the reason.
+template <class T, int AX>
+PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  T WL[NV8], WR[NV8], FL[NV8], FR[NV8];
+  cons_to_prim<T, AX>(UL, WL, ph);
+  cons_to_prim<T, AX>(UR, WR, ph);
+  phys_flux<T, AX>(WL, UL[EN], FL);
+  phys_flux<T, AX>(WR, UR[EN], FR);
+  const T cfL = fast_speed<T, AX>(WL, ph);
+  const T cfR = fast_speed<T, AX>(WR, ph);
+  const T sL = vmin(WL[D::vn] - cfL, WR[D::vn] - cfR);
+  const T sR = vmax(WL[D::vn] + cfL, WR[D::vn] + cfR);
+  if (sL >= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FL[k];
+    return HLLD_OK;
+  }
+  if (sR <= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FR[k];
+    return HLLD_OK;
+  }
+  const T rhoL = vmax(WL[RHO], rho_floor<T>());
+  const T rhoR = vmax(WR[RHO], rho_floor<T>());
+  const T vnL = WL[D::vn], vnR = WR[D::vn];
+  const T bn = (T)0.5 * (WL[D::bn] + WR[D::bn]);
+  const T b2L = bn * bn + WL[D::bt1] * WL[D::bt1] + WL[D::bt2] * WL[D::bt2];
+  const T b2R = bn * bn + WR[D::bt1] * WR[D::bt1] + WR[D::bt2] * WR[D::bt2];
+  const T ptL = vmax(WL[EN], p_floor<T>()) + (T)0.5 * b2L;
+  const T ptR = vmax(WR[EN], p_floor<T>()) + (T)0.5 * b2R;
+  const T denom_sm = rhoR * (sR - vnR) - rhoL * (sL - vnL);
+  const T denom_sm_scale = vabs(rhoR * (sR - vnR)) + vabs(rhoL * (sL - vnL));
+  const T b_scale = vsqrt(vmax(b2L, b2R));
+  if (hlld_small(denom_sm, denom_sm_scale, ph) || hlld_small(bn, b_scale, ph)) {
+    hll_flux<T, AX>(UL, UR, F, ph);
+    return HLLD_FALLBACK_DEGENERATE;
+  }
+  const T sm = (rhoR * vnR * (sR - vnR) - rhoL * vnL * (sL - vnL) + ptL - ptR) / denom_sm;
+  const T ptsL = ptL + rhoL * (sL - vnL) * (sm - vnL);
+  const T ptsR = ptR + rhoR * (sR - vnR) * (sm - vnR);
+  const T pts = (T)0.5 * (ptsL + ptsR);
+  T ULs[NV8], URs[NV8];
+  const int stL = hlld_star<T, AX>(UL, WL, sL, sm, pts, bn, ULs, ph);
+  const int stR = hlld_star<T, AX>(UR, WR, sR, sm, pts, bn, URs, ph);
+  if (stL != HLLD_OK || stR != HLLD_OK) {
+    hll_flux<T, AX>(UL, UR, F, ph);
+    return (stL != HLLD_OK) ? stL : stR;
+  }
+  const T sqL = vsqrt(vmax(ULs[RHO], rho_floor<T>()));
+  const T sqR = vsqrt(vmax(URs[RHO], rho_floor<T>()));
+  const T sgn = (bn < (T)0.0) ? (T)-1.0 : (T)1.0;
+  const T sLs = sm - vabs(bn) / sqL;
+  const T sRs = sm + vabs(bn) / sqR;
+  const T den = sqL + sqR;
+  if (den <= (T)0.0) {
+    hll_flux<T, AX>(UL, UR, F, ph);
+    return HLLD_FALLBACK_DEGENERATE;
+  }
+  const T vt1Ls = ULs[D::vt1] / ULs[RHO], vt2Ls = ULs[D::vt2] / ULs[RHO];
+  const T bt1Ls = ULs[D::bt1], bt2Ls = ULs[D::bt2];
+  const T vt1Rs = URs[D::vt1] / URs[RHO], vt2Rs = URs[D::vt2] / URs[RHO];
+  const T bt1Rs = URs[D::bt1], bt2Rs = URs[D::bt2];
+  const T vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) / den;
+  const T vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) / den;
+  const T bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) / den;
+  const T bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) / den;
+  // Double-star states differ from the star states only in the tangential
+  // slots and the energy.
+  T ULD[NV8], URD[NV8];
+#pragma unroll
+  for (int k = 0; k < NV8; k++) {
+    ULD[k] = ULs[k];
+    URD[k] = URs[k];
+  }
+  ULD[D::vt1] = ULD[RHO] * vt1D;
+  ULD[D::vt2] = ULD[RHO] * vt2D;
+  ULD[D::bt1] = bt1D;
+  ULD[D::bt2] = bt2D;
+  URD[D::vt1] = URD[RHO] * vt1D;
+  URD[D::vt2] = URD[RHO] * vt2D;
+  URD[D::bt1] = bt1D;
+  URD[D::bt2] = bt2D;
+  const T vbD = sm * bn + vt1D * bt1D + vt2D * bt2D;
+  const T vbLs = sm * bn + vt1Ls * bt1Ls + vt2Ls * bt2Ls;
+  const T vbRs = sm * bn + vt1Rs * bt1Rs + vt2Rs * bt2Rs;
+  ULD[EN] = ULs[EN] - sgn * sqL * (vbLs - vbD);
+  URD[EN] = URs[EN] + sgn * sqR * (vbRs - vbD);
+  if (!positive_state<T, AX>(ULD, ph) || !positive_state<T, AX>(URD, ph)) {
+    hll_flux<T, AX>(UL, UR, F, ph);
+    return HLLD_FALLBACK_NONPHYSICAL;
+  }
+  if (sLs >= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FL[k] + sL * (ULs[k] - UL[k]);
+  } else if (sm >= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FL[k] + sL * (ULs[k] - UL[k]) + sLs * (ULD[k] - ULs[k]);
+  } else if (sRs >= (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FR[k] + sR * (URs[k] - UR[k]) + sRs * (URD[k] - URs[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV8; k++) F[k] = FR[k] + sR * (URs[k] - UR[k]);
+  }
+  return HLLD_OK;
+}
+
+// Mixed-GLM interface flux along AX (mhdGlmNormalState + mhdGlmFluxX/Y,
+// mhd_glm_common.hpp:55-126): upwind B_n* and psi* of the linear GLM
+// subsystem, HLLD (or HLL) on the 8 MHD slots with B_n = B_n* on both sides,
+// F[B_n] = psi*, F[psi] = ch^2 B_n*.
+template <class T, int AX>
+PMHD_HD int glm_flux(const T* UL, const T* UR, T ch, bool use_hlld, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T ch_safe = vmax(ch, (T)1.0e-12);
+  const T bnL = UL[D::bn], bnR = UR[D::bn], psiL = UL[PSI], psiR = UR[PSI];
+  const T bns = (T)0.5 * (bnL + bnR) - (T)0.5 * (psiR - psiL) / ch_safe;
+  const T psis = (T)0.5 * (psiL + psiR) - (T)0.5 * ch_safe * (bnR - bnL);
+  T a[NV8], b[NV8];
+#pragma unroll
+  for (int k = 0; k < NV8; k++) {
+    a[k] = UL[k];
+    b[k] = UR[k];
+  }
+  a[D::bn] = bns;
+  b[D::bn] = bns;
+  int status = HLLD_OK;
+  if (use_hlld)
+    status = hlld_flux<T, AX>(a, b, F, ph);
+  else
+    hll_flux<T, AX>(a, b, F, ph);
+  F[D::bn] = psis;
+  F[PSI] = ch * ch * bns;
+  return status;
+}
+
+// ---- 9-slot helpers of the 2D driver (mhd2d_glm_cpu.cpp:90-161) ----------
+
+// Conserved -> primitive with psi carried in slot 8.
+template <class T>
+PMHD_HD void state_to_prim9(const T* U, T* P, const Phys<T>& ph) {
+  cons_to_prim<T, 0>(U, P, ph);
+  P[PSI] = U[PSI];
+}
+
+template <class T>
+PMHD_HD void prim9_to_state(const T* P, T* U, const Phys<T>& ph) {
+  prim_to_cons<T>(P, U, ph);
+  U[PSI] = P[PSI];
+}
+
+// Positive floors and all nine slots finite (primitiveIsUsable).
+template <class T>
+PMHD_HD bool prim9_usable(const T* P) {
+  if (P[RHO] <= rho_floor<T>() || P[EN] <= p_floor<T>()) return false;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < NV9; k++) ok = ok && vfinite(P[k]);
+  return ok;
+}
+
+// stateIsUsable: density above the floor before recovery, then the
+// primitive test.
+template <class T>
+PMHD_HD bool state_usable(const T* U, const Phys<T>& ph) {
+  if (U[RHO] <= rho_floor<T>()) return false;
+  T P[NV9];
+  state_to_prim9<T>(U, P, ph);
+  return prim9_usable<T>(P);
+}
+
+// Limited linear reconstruction of one cell from its two neighbours along an
+// axis: Pl = left face, Pr = right face; first order when either face is
+// unusable (reconstructPrimitive).
+template <class T>
+PMHD_HD void recon_cell(const T* Pm, const T* P0, const T* Pp, T* Pl, T* Pr) {
+#pragma unroll
+  for (int k = 0; k < NV9; k++) {
+    const T slope = minmod(P0[k] - Pm[k], Pp[k] - P0[k]);
+    Pl[k] = P0[k] - (T)0.5 * slope;
+    Pr[k] = P0[k] + (T)0.5 * slope;
+  }
+  if (!prim9_usable<T>(Pl) || !prim9_usable<T>(Pr)) {
+#pragma unroll
+    for (int k = 0; k < NV9; k++) {
+      Pl[k] = P0[k];
+      Pr[k] = P0[k];
+    }
+  }
+}
+
+// Signal speed of one cell, max(|vx| + cf_x, |vy| + cf_y).
+template <class T>
+PMHD_HD T cell_speed(const T* P, const Phys<T>& ph) {
+  const T sx = vabs(P[MX]) + fast_speed<T, 0>(P, ph);
+  const T sy = vabs(P[MY]) + fast_speed<T, 1>(P, ph);
+  return vmax(sx, sy);
+}
+
+}  // namespace pmhd
+
+#endif  // PMHD_POINT_HPP

@@ -1,0 +1,217 @@
+// mhd2d_glm_gpu -- drop-in replacement for the reference program of the same
+// name (src/mhd/mhd2d_glm_gpu.cu, main at :353-653), running on libpmhd.so.
+//
+//   mhd2d_glm_gpu [nx ny t_end cfl {muscl|first} {hll|hlld} alpha [ot|kh]]
+//
+// Same positional arguments and defaults (128 128 0.5 0.25 muscl hlld 0.18
+// ot), the same stdout summary lines that the reference's scripts grep, the
+// same .dat file under $OUTDIR (default results/mhd/gpu/<problem>) and the
+// same exit codes (1 bad arguments, 2 non-positive rate, 3 / 4 non-physical
+// stage, 5 cannot open the output, 9 CUDA error).
+//
+// The reference selects the precision at compile time (separate fp64, fp32
+// and mixed binaries); here the program name picks it: a name ending in
+// "_fp32" or "_mixed" runs that precision, anything else fp64, and the
+// environment variable PMHD_PRECISION (fp64|fp32|mixed) overrides the name.
+// PMHD_EXACT=1 selects the kernels built without FMA contraction, whose fp64
+// output is bit-identical to the reference CPU build.
+// Extensions: problem "kh_reflect" (single shear layer on [0,1]x[-1,1], y
+// reflecting walls) and "brio_wu" (rotated Brio-Wu tube, gamma 2,
+// transmissive walls; alpha doubles as the interface angle in degrees is
+// NOT done -- the angle comes from PMHD_ANGLE, radians).
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <string>
+
+#include "pmhd.h"
+
+static bool ends_with(const std::string& s, const std::string& suf) {
+  return s.size() >= suf.size() && s.compare(s.size() - suf.size(), suf.size(), suf) == 0;
+}
+
+int main(int argc, char* argv[]) {
+  pmhd_config cfg;
+  pmhd_config_default(&cfg);
+  int nx = 128, ny = 128;
+  double t_end = 0.5, cfl = 0.25, alpha = 0.18;
+  std::string order = "muscl", solver = "hlld", problem = "ot";
+  if (argc > 1) nx = std::atoi(argv[1]);
+  if (argc > 2) ny = std::atoi(argv[2]);
+  if (argc > 3) t_end = std::atof(argv[3]);
+  if (argc > 4) cfl = std::atof(argv[4]);
+  if (argc > 5) order = argv[5];
+  if (argc > 6) solver = argv[6];
+  if (argc > 7) alpha = std::atof(argv[7]);
+  if (argc > 8) problem = argv[8];
+
+  std::string prog = argv[0];
+  int precision = PMHD_FP64;
+  if (ends_with(prog, "_fp32")) precision = PMHD_FP32;
+  if (ends_with(prog, "_mixed")) precision = PMHD_MIXED;
+  if (const char* e = std::getenv("PMHD_PRECISION")) {
+    std::string v = e;
+    if (v == "fp32") precision = PMHD_FP32;
+    else if (v == "mixed") precision = PMHD_MIXED;
+    else if (v == "fp64") precision = PMHD_FP64;
+    else {
+      std::cerr << "Error: PMHD_PRECISION must be fp64, fp32 or mixed." << std::endl;
+      return 1;
+    }
+  }
+  const bool f32 = precision == PMHD_FP32;
+  // Values the reference holds in its Real type.
+  auto real = [&](double v) { return f32 ? (double)(float)v : v; };
+
+  if (problem != "ot" && problem != "kh" && problem != "kh_reflect" && problem != "brio_wu") {
+    std::cerr << "Error: problem must be 'ot' or 'kh'." << std::endl;
+    return 1;
+  }
+  if (order != "muscl" && order != "first") {
+    std::cerr << "Error: order must be 'muscl' or 'first'." << std::endl;
+    return 1;
+  }
+  if (solver != "hll" && solver != "hlld") {
+    std::cerr << "Error: solver must be 'hll' or 'hlld'." << std::endl;
+    return 1;
+  }
+  if (!(real(alpha) > 0.0)) {
+    std::cerr << "Error: alpha must be positive." << std::endl;
+    return 1;
+  }
+  cfg.nx = nx;
+  cfg.ny = ny;
+  cfg.cfl = cfl;
+  cfg.alpha = alpha;
+  cfg.order = order == "muscl" ? PMHD_ORDER_MUSCL : PMHD_ORDER_FIRST;
+  cfg.solver = solver == "hlld" ? PMHD_SOLVER_HLLD : PMHD_SOLVER_HLL;
+  cfg.precision = precision;
+  if (const char* e = std::getenv("PMHD_EXACT")) cfg.exact = std::atoi(e) != 0;
+  if (const char* e = std::getenv("MHD_HLLD_TOLERANCE")) cfg.hlld_tol = std::atof(e);
+  int prob_id = PMHD_PROBLEM_ORSZAG_TANG;
+  double params[1] = {0.0};
+  int nparams = 0;
+  if (problem == "kh") prob_id = PMHD_PROBLEM_KH_REF;
+  if (problem == "kh_reflect") {
+    prob_id = PMHD_PROBLEM_KH_REFLECT;
+    cfg.y_min = -1.0;
+    cfg.y_max = 1.0;
+    cfg.bc[2] = cfg.bc[3] = PMHD_BC_REFLECT;
+  }
+  if (problem == "brio_wu") {
+    prob_id = PMHD_PROBLEM_BRIO_WU_2D;
+    cfg.gamma = 2.0;
+    for (int k = 0; k < 4; k++) cfg.bc[k] = PMHD_BC_TRANSMISSIVE;
+    if (const char* e = std::getenv("PMHD_ANGLE")) params[0] = std::atof(e);
+    nparams = 1;
+  }
+
+  std::cout << "===== 2D ideal MHD Orszag-Tang vortex with mixed GLM (GPU) =====" << std::endl;
+  std::cout << "Solver: " << (cfg.solver == PMHD_SOLVER_HLLD ? "HLLD" : "HLL") << std::endl;
+  std::cout << "Reconstruction/time: "
+            << (cfg.order == PMHD_ORDER_MUSCL ? "MUSCL + SSPRK2" : "first-order + SSPRK2") << std::endl;
+  std::cout << "Precision: " << (f32 ? 32 : 64) << " bit" << (f32 ? " (fp32)" : " (fp64)")
+            << (precision == PMHD_MIXED ? " storage, fp32 flux (mixed)" : "") << std::endl;
+  if (f32)
+    std::cout << "gamma = " << (float)cfg.gamma << ", alpha = " << (float)alpha << std::endl;
+  else
+    std::cout << "gamma = " << cfg.gamma << ", alpha = " << alpha << std::endl;
+  if (f32)
+    std::cout << "Nx x Ny = " << nx << " x " << ny << ", CFL = " << (float)cfl << ", t_end = " << (float)t_end
+              << std::endl;
+  else
+    std::cout << "Nx x Ny = " << nx << " x " << ny << ", CFL = " << cfl << ", t_end = " << t_end << std::endl;
+
+  pmhd_solver* s = nullptr;
+  int rc = pmhd_create(&cfg, &s);
+  if (rc != PMHD_OK) {
+    std::cerr << "Error: " << pmhd_strerror(rc) << std::endl;
+    return rc == PMHD_ERR_ARG ? 1 : 9;
+  }
+  rc = pmhd_init_problem(s, prob_id, nparams ? params : nullptr, nparams);
+  if (rc != PMHD_OK) {
+    std::cerr << "Error: " << pmhd_strerror(rc) << std::endl;
+    pmhd_destroy(s);
+    return 9;
+  }
+
+  pmhd_stats st;
+  auto t0 = std::chrono::steady_clock::now();
+  rc = pmhd_advance(s, t_end, -1, &st);
+  auto t1 = std::chrono::steady_clock::now();
+  const double wall = std::chrono::duration<double>(t1 - t0).count();
+  if (rc == PMHD_ERR_STAGE1 || rc == PMHD_ERR_STAGE2) {
+    std::cerr << (rc == PMHD_ERR_STAGE1 ? "Error: non-physical RK stage at step "
+                                        : "Error: non-physical state at step ")
+              << st.bad_step << ", cell (" << st.bad_i << ", " << st.bad_j << ")" << std::endl;
+    pmhd_destroy(s);
+    return rc;
+  }
+  if (rc != PMHD_OK) {
+    std::cerr << "Error: " << pmhd_strerror(rc) << std::endl;
+    pmhd_destroy(s);
+    return rc == PMHD_ERR_RATE ? 2 : 9;
+  }
+
+  auto pr = [&](double v) -> std::ostream& {
+    if (f32) return std::cout << (float)v;
+    return std::cout << v;
+  };
+  std::cout << "Done. Steps: " << st.steps << ", final t = ";
+  pr(st.t) << std::endl;
+  std::cout << "c_h(last) = ";
+  pr(st.ch_last) << ", alpha = ";
+  pr(alpha) << std::endl;
+  std::cout << "Time loop wall time = " << std::fixed << std::setprecision(3) << wall << " s ("
+            << std::setprecision(2) << ((double)nx * ny * st.steps / wall / 1.0e6) << " Mcell-steps/s)"
+            << std::defaultfloat << std::endl;
+  double diag[3];
+  if (pmhd_diagnostics(s, diag) != PMHD_OK) {
+    pmhd_destroy(s);
+    return 9;
+  }
+  std::cout << "divB L1 = ";
+  pr(diag[0]) << ", divB Linf = ";
+  pr(diag[1]) << ", psi Linf = ";
+  pr(diag[2]) << std::endl;
+  if (cfg.solver == PMHD_SOLVER_HLLD) {
+    const unsigned long long evals = st.x_evals + st.y_evals;
+    const unsigned long long fb = st.degenerate + st.nonphysical;
+    const double frac = evals > 0 ? (double)fb / (double)evals : 0.0;
+    std::cout << "HLLD flux evaluations = " << evals << " (x=" << st.x_evals << ", y=" << st.y_evals << ")"
+              << std::endl;
+    std::cout << "HLLD relative fallback tolerance = " << std::scientific << (double)real(cfg.hlld_tol)
+              << std::defaultfloat << std::endl;
+    std::cout << "HLLD->HLL fallbacks = " << fb << " (degenerate=" << st.degenerate
+              << ", nonphysical=" << st.nonphysical << "), fraction = " << std::scientific << frac
+              << std::defaultfloat << std::endl;
+  }
+
+  const char* out_env = std::getenv("OUTDIR");
+  const std::string prob_base = problem == "ot" ? "orszag_tang" : problem;
+  const std::string out_dir = out_env ? std::string(out_env) : std::string("results/mhd/gpu/") + prob_base;
+  const std::string mk = "mkdir -p '" + out_dir + "'";
+  if (std::system(mk.c_str()) != 0) { /* the open below reports the failure */ }
+  char fname[512];
+  pmhd_dat_filename(s, prob_base.c_str(), fname, sizeof(fname));
+  const std::string path = out_dir + "/" + fname;
+  const std::string title = problem == "kh" ? "Kelvin-Helmholtz ideal MHD with mixed GLM (GPU)"
+                                            : (problem == "ot" ? "Orszag-Tang ideal MHD with mixed GLM (GPU)"
+                                                               : problem + " ideal MHD with mixed GLM (GPU)");
+  rc = pmhd_write_dat(s, path.c_str(), title.c_str());
+  if (rc == PMHD_ERR_IO) {
+    std::cerr << "Error: failed to open output file: " << path << std::endl;
+    pmhd_destroy(s);
+    return 5;
+  }
+  if (rc != PMHD_OK) {
+    pmhd_destroy(s);
+    return 9;
+  }
+  std::cout << "Saved: " << path << std::endl;
+  pmhd_destroy(s);
+  return 0;
+}

@@ -1,0 +1,247 @@
+"""Python bindings (ctypes) for libpmhd.so, the B200 2D ideal-MHD + GLM solver.
+
+The C ABI is declared in include/pmhd.h.  This module loads the in-tree
+library built by precision-study_b200/Makefile and fails loudly when it is
+missing: there is no CPU fallback.
+
+Typical use::
+
+    import pmhd
+    with pmhd.Solver(nx=256, ny=256, precision="mixed") as s:
+        s.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
+        st = s.advance(t_end=0.5)
+        U = s.get_state()            # (ny, nx, 9) conserved fields
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libpmhd.so")
+CLI_PATH = os.path.join(PKG_DIR, "bin", "mhd2d_glm_gpu")
+
+OK, ERR_ARG, ERR_RATE, ERR_STAGE1, ERR_STAGE2, ERR_IO, ERR_CUDA = 0, 1, 2, 3, 4, 5, 9
+ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE = -1, -2, -3, -4
+FP64, FP32, MIXED = 0, 1, 2
+BC_PERIODIC, BC_REFLECT, BC_TRANSMISSIVE = 0, 1, 2
+ORDER_FIRST, ORDER_MUSCL = 0, 1
+SOLVER_HLL, SOLVER_HLLD = 0, 1
+PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D = 0, 1, 2, 3
+LAYOUT_INTERIOR, LAYOUT_GHOSTED = 0, 1
+
+PRECISIONS = {"fp64": FP64, "fp32": FP32, "mixed": MIXED}
+
+# Every entry point include/pmhd.h declares.
+EXPORTS = (
+    "pmhd_config_default", "pmhd_create", "pmhd_destroy", "pmhd_init_problem",
+    "pmhd_set_state", "pmhd_get_state", "pmhd_set_time", "pmhd_advance",
+    "pmhd_get_stats", "pmhd_diagnostics", "pmhd_write_dat", "pmhd_dat_filename",
+    "pmhd_strerror", "pmhd_get_config",
+)
+
+
+class PmhdError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        super().__init__(f"{where}: {strerror(status)} (status {status})")
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+        ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("hlld_tol", ctypes.c_double),
+        ("cfl", ctypes.c_double), ("alpha", ctypes.c_double),
+        ("order", ctypes.c_int), ("solver", ctypes.c_int),
+        ("precision", ctypes.c_int), ("exact", ctypes.c_int),
+        ("bc", ctypes.c_int * 4), ("device", ctypes.c_int),
+        ("steps_per_graph", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_longlong), ("t", ctypes.c_double),
+        ("ch_last", ctypes.c_double), ("dt_last", ctypes.c_double),
+        ("x_evals", ctypes.c_ulonglong), ("y_evals", ctypes.c_ulonglong),
+        ("degenerate", ctypes.c_ulonglong), ("nonphysical", ctypes.c_ulonglong),
+        ("status", ctypes.c_int), ("bad_i", ctypes.c_int), ("bad_j", ctypes.c_int),
+        ("bad_step", ctypes.c_longlong), ("kernel_launches", ctypes.c_ulonglong),
+        ("device_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load():
+    """Load libpmhd.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, vp, i, d = ctypes.POINTER, ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "pmhd_config_default": ([P(Config)], i),
+        "pmhd_create": ([P(Config), P(vp)], i),
+        "pmhd_destroy": ([vp], i),
+        "pmhd_init_problem": ([vp, i, P(d), i], i),
+        "pmhd_set_state": ([vp, vp, i], i),
+        "pmhd_get_state": ([vp, vp, i], i),
+        "pmhd_set_time": ([vp, d, ctypes.c_longlong], i),
+        "pmhd_advance": ([vp, d, ctypes.c_longlong, P(Stats)], i),
+        "pmhd_get_stats": ([vp, P(Stats)], i),
+        "pmhd_diagnostics": ([vp, P(d)], i),
+        "pmhd_write_dat": ([vp, ctypes.c_char_p, ctypes.c_char_p], i),
+        "pmhd_dat_filename": ([vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t], i),
+        "pmhd_strerror": ([i], ctypes.c_char_p),
+        "pmhd_get_config": ([vp, P(Config)], i),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def strerror(status):
+    return load().pmhd_strerror(status).decode()
+
+
+def default_config():
+    c = Config()
+    load().pmhd_config_default(ctypes.byref(c))
+    return c
+
+
+def _check(status, where):
+    if status != OK:
+        raise PmhdError(status, where)
+
+
+class Solver:
+    """One grid on one GPU (a pmhd_solver handle)."""
+
+    def __init__(self, nx=128, ny=128, precision="fp64", exact=False, order="muscl",
+                 solver="hlld", cfl=0.25, alpha=0.18, gamma=5.0 / 3.0, hlld_tol=1e-4,
+                 domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0), device=0, steps_per_graph=0):
+        L = load()
+        c = default_config()
+        c.nx, c.ny = nx, ny
+        c.x_min, c.x_max, c.y_min, c.y_max = domain
+        c.gamma, c.hlld_tol, c.cfl, c.alpha = gamma, hlld_tol, cfl, alpha
+        c.order = ORDER_MUSCL if order == "muscl" else ORDER_FIRST
+        c.solver = SOLVER_HLLD if solver == "hlld" else SOLVER_HLL
+        c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        c.exact = int(bool(exact))
+        for k in range(4):
+            c.bc[k] = bc[k]
+        c.device = device
+        c.steps_per_graph = steps_per_graph
+        self.cfg = c
+        self.dtype = np.float32 if c.precision == FP32 else np.float64
+        h = ctypes.c_void_p()
+        _check(L.pmhd_create(ctypes.byref(c), ctypes.byref(h)), "pmhd_create")
+        self._h = h
+
+    # context manager / lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pmhd_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _shape(self, layout):
+        c = self.cfg
+        return (c.ny, c.nx, 9) if layout == LAYOUT_INTERIOR else (c.ny + 4, c.nx + 4, 9)
+
+    def init_problem(self, problem, params=None):
+        arr = None
+        n = 0
+        if params is not None:
+            n = len(params)
+            arr = (ctypes.c_double * n)(*params)
+        _check(load().pmhd_init_problem(self._h, problem, arr, n), "pmhd_init_problem")
+
+    def set_state(self, U, layout=LAYOUT_INTERIOR):
+        U = np.ascontiguousarray(U, dtype=self.dtype)
+        assert U.shape == self._shape(layout), (U.shape, self._shape(layout))
+        _check(load().pmhd_set_state(self._h, U.ctypes.data, layout), "pmhd_set_state")
+
+    def get_state(self, layout=LAYOUT_INTERIOR, out=None):
+        if out is None:
+            out = np.empty(self._shape(layout), dtype=self.dtype)
+        assert out.shape == self._shape(layout) and out.dtype == self.dtype and out.flags["C_CONTIGUOUS"]
+        _check(load().pmhd_get_state(self._h, out.ctypes.data, layout), "pmhd_get_state")
+        return out
+
+    def set_time(self, t, steps=0):
+        _check(load().pmhd_set_time(self._h, t, steps), "pmhd_set_time")
+
+    def advance(self, t_end=float("inf"), max_steps=-1, check=True):
+        st = Stats()
+        rc = load().pmhd_advance(self._h, t_end, max_steps, ctypes.byref(st))
+        if check:
+            _check(rc, "pmhd_advance")
+        return st
+
+    def stats(self):
+        st = Stats()
+        _check(load().pmhd_get_stats(self._h, ctypes.byref(st)), "pmhd_get_stats")
+        return st
+
+    def diagnostics(self):
+        out = (ctypes.c_double * 3)()
+        _check(load().pmhd_diagnostics(self._h, out), "pmhd_diagnostics")
+        return tuple(out)
+
+    def write_dat(self, path, title=None):
+        _check(load().pmhd_write_dat(self._h, path.encode(), title.encode() if title else None),
+               "pmhd_write_dat")
+
+    def dat_filename(self, prob_base="orszag_tang"):
+        buf = ctypes.create_string_buffer(512)
+        _check(load().pmhd_dat_filename(self._h, prob_base.encode(), buf, 512), "pmhd_dat_filename")
+        return buf.value.decode()
+
+
+def relative_l2(ref, other):
+    """Per-variable relative L2 = RMS(ref - other) / RMS(ref), the metric of
+    the reference's analysis/mhd/compare_precision.py:51-58, over the last
+    axis of (..., nvar) arrays."""
+    ref = np.asarray(ref, dtype=np.float64).reshape(-1, ref.shape[-1])
+    other = np.asarray(other, dtype=np.float64).reshape(-1, ref.shape[-1])
+    d = ref - other
+    l2 = np.sqrt(np.mean(d * d, axis=0))
+    rms = np.sqrt(np.mean(ref * ref, axis=0))
+    return np.where(rms > 0, l2 / np.where(rms > 0, rms, 1.0), 0.0)
+
+
+def conserved_to_dat_columns(U, gamma=5.0 / 3.0):
+    """Primitive columns (rho vx vy vz p Bx By Bz E) of a (..., 9) conserved
+    array, as the reference .dat file lists them."""
+    U = np.asarray(U, dtype=np.float64)
+    rho = np.maximum(U[..., 0], 1e-12)
+    vx, vy, vz = U[..., 1] / rho, U[..., 2] / rho, U[..., 3] / rho
+    bx, by, bz = U[..., 5], U[..., 6], U[..., 7]
+    p = (gamma - 1.0) * (U[..., 4] - 0.5 * rho * (vx * vx + vy * vy + vz * vz) - 0.5 * (bx * bx + by * by + bz * bz))
+    return np.stack([rho, vx, vy, vz, p, bx, by, bz, U[..., 4]], axis=-1)

@@ -1,0 +1,178 @@
+"""GPU parity of the fused sm_100a stage kernels against the CPU oracle and
+the reference's published known answers.
+
+Bar (stated per test):
+  * exact mode (kernels built with -fmad=false): bit-identical to the oracle
+    for every precision policy, and, for fp64/fp32, to the reference CPU
+    build's output files and HLLD fallback counts;
+  * FMA mode: relative L2 <= 1e-12 per conserved variable for fp64 at short
+    times (rounding differences grow chaotically over long runs); for
+    fp32/mixed <= 1e-5 on the eight MHD variables and <= 1e-3 on psi, the
+    cleaning field, which is driven by discretisation noise and so is far
+    more sensitive to rounding than the physical fields.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PREC_OF = {"fp64": "f64", "fp32": "f32", "mixed": "mixed"}
+
+
+def gpu_run(pmhd, prec, nx, ny, t_end, exact=True, order="muscl", solver="hlld", problem=0,
+            max_steps=-1, alpha=0.18, cfl=0.25, domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0),
+            gamma=5.0 / 3.0, params=None, U0=None):
+    with pmhd.Solver(nx=nx, ny=ny, precision=prec, exact=exact, order=order, solver=solver,
+                     alpha=alpha, cfl=cfl, domain=domain, bc=bc, gamma=gamma) as s:
+        if U0 is None:
+            s.init_problem(problem, params)
+        else:
+            s.set_state(U0, layout=pmhd.LAYOUT_GHOSTED)
+        st = s.advance(t_end=t_end, max_steps=max_steps)
+        U = s.get_state(layout=pmhd.LAYOUT_GHOSTED)
+    return U, st
+
+
+def oracle_run(oracle, prec, nx, ny, t_end, order="muscl", solver="hlld", problem=0, max_steps=-1,
+               alpha=0.18, cfl=0.25, domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0), gamma=5.0 / 3.0,
+               U0=None):
+    cfg = oracle.make_config(nx, ny, t_end, cfl=cfl, alpha=alpha, muscl=(order == "muscl"),
+                             hlld=(solver == "hlld"), gamma=gamma, domain=domain, bc=bc,
+                             max_steps=max_steps)
+    if U0 is None:
+        U = oracle.init_ref_problem("f32" if prec == "fp32" else "f64", problem, nx, ny, domain, gamma)
+    else:
+        U = np.array(U0, copy=True)
+    st = oracle.run(PREC_OF[prec], cfg, U)
+    return U, st
+
+
+def interior(U):
+    return U[2:-2, 2:-2, :]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+@pytest.mark.parametrize("order,solver", [("muscl", "hlld"), ("first", "hll"), ("muscl", "hll"),
+                                          ("first", "hlld")])
+def test_exact_bitwise_vs_oracle_ot(pmhd_lib, oracle, prec, order, solver):
+    nx, ny, t_end = 40, 24, 0.06
+    Ug, sg = gpu_run(pmhd_lib, prec, nx, ny, t_end, order=order, solver=solver)
+    Uo, so = oracle_run(oracle, prec, nx, ny, t_end, order=order, solver=solver)
+    assert sg.status == 0 and so.status == 0
+    assert sg.steps == so.steps and sg.t == so.t
+    assert sg.ch_last == so.ch_last
+    assert (sg.degenerate, sg.nonphysical) == (so.degenerate, so.nonphysical)
+    assert (sg.x_evals, sg.y_evals) == (so.x_evals, so.y_evals)
+    np.testing.assert_array_equal(interior(Ug), interior(Uo))
+    np.testing.assert_array_equal(Ug, Uo)  # ghost layers (incl. corners) too
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+def test_exact_bitwise_vs_oracle_kh_ref(pmhd_lib, oracle, prec):
+    nx, ny, t_end = 48, 48, 0.05
+    Ug, sg = gpu_run(pmhd_lib, prec, nx, ny, t_end, problem=1)
+    Uo, so = oracle_run(oracle, prec, nx, ny, t_end, problem=1)
+    assert sg.steps == so.steps and sg.t == so.t
+    assert (sg.degenerate, sg.nonphysical) == (so.degenerate, so.nonphysical)
+    np.testing.assert_array_equal(Ug, Uo)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_exact_bitwise_nonperiodic_partial_tiles(pmhd_lib, oracle, prec):
+    """Reflecting y walls, transmissive x walls and a grid that is not a
+    multiple of the 32 x 8 tile (partial tiles on both axes)."""
+    nx, ny = 45, 21
+    bc = (2, 2, 1, 1)
+    domain = (0.0, 1.0, -1.0, 1.0)
+    U0 = np.zeros((ny + 4, nx + 4, 9))
+    with pmhd_lib.Solver(nx=nx, ny=ny, precision=prec, exact=True, domain=domain, bc=bc) as s:
+        s.init_problem(pmhd_lib.PROBLEM_KH_REFLECT, [0.08, 0.1])
+        U0 = s.get_state(layout=pmhd_lib.LAYOUT_GHOSTED)
+    Ug, sg = gpu_run(pmhd_lib, prec, nx, ny, 0.08, domain=domain, bc=bc, U0=U0)
+    Uo, so = oracle_run(oracle, prec, nx, ny, 0.08, domain=domain, bc=bc, U0=U0)
+    assert sg.steps == so.steps > 3
+    assert (sg.degenerate, sg.nonphysical) == (so.degenerate, so.nonphysical)
+    np.testing.assert_array_equal(Ug, Uo)
+
+
+def test_exact_step_limit_and_resume(pmhd_lib, oracle):
+    """max_steps stops exactly; a second advance continues bit-identically."""
+    nx = ny = 32
+    with pmhd_lib.Solver(nx=nx, ny=ny, precision="fp64", exact=True) as s:
+        s.init_problem(0)
+        st1 = s.advance(t_end=0.1, max_steps=7)
+        assert st1.steps == 7
+        st2 = s.advance(t_end=0.1)
+        Ug = s.get_state(layout=pmhd_lib.LAYOUT_GHOSTED)
+    Uo, so = oracle_run(oracle, "fp64", nx, ny, 0.1)
+    assert st2.steps == so.steps and st2.t == so.t
+    assert st2.degenerate == so.degenerate
+    np.testing.assert_array_equal(Ug, Uo)
+
+
+def _md5_data_lines(path):
+    h = hashlib.md5()
+    with open(path, "rb") as f:
+        for line in f:
+            if not line.startswith(b"#"):
+                h.update(line)
+    return h.hexdigest()
+
+
+# Known answers of the reference CPU build at OT 192^2, t = 0.5, eps = 1e-4
+# (logs/mhd/ot_large_eps1e-4_20260715/mhd2d_fp{64,32}_eps1e-4_N192.log and
+# the data-line md5 of its .dat output, reproduced in tests/golden).
+OT192 = {
+    "fp64": dict(steps=1936, degenerate=13370, nonphysical=2, md5="4fe78b53eebc633b94d04b01b37ebbca"),
+    "fp32": dict(steps=1936, degenerate=13362, nonphysical=2, md5="dfa6392909b0b20979fa4a45b9a1334d"),
+}
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_exact_ot192_matches_reference_output(pmhd_lib, prec, tmp_path):
+    ka = OT192[prec]
+    with pmhd_lib.Solver(nx=192, ny=192, precision=prec, exact=True) as s:
+        s.init_problem(0)
+        st = s.advance(t_end=0.5)
+        path = str(tmp_path / s.dat_filename())
+        s.write_dat(path)
+    assert st.steps == ka["steps"]
+    assert (st.degenerate, st.nonphysical) == (ka["degenerate"], ka["nonphysical"])
+    assert st.x_evals == st.y_evals == 143480832
+    assert _md5_data_lines(path) == ka["md5"]
+
+
+# Reference CPU logs logs/mhd/ot_large_eps1e-4_20260715/ot_fp{64,32}_N{256,384,512}.log
+OT_LARGE = [
+    ("fp64", 256, 2595, 37374, 8), ("fp64", 384, 3917, 144924, 4), ("fp64", 512, 5239, 374612, 20),
+    ("fp32", 256, 2595, 37396, 7), ("fp32", 384, 3917, 145077, 7), ("fp32", 512, 5239, 374636, 11),
+]
+
+
+@pytest.mark.parametrize("prec,n,steps,deg,nonphys", OT_LARGE)
+def test_exact_ot_large_fallback_counts(pmhd_lib, prec, n, steps, deg, nonphys):
+    with pmhd_lib.Solver(nx=n, ny=n, precision=prec, exact=True) as s:
+        s.init_problem(0)
+        st = s.advance(t_end=0.5)
+    assert st.steps == steps
+    assert (st.degenerate, st.nonphysical) == (deg, nonphys)
+
+
+FMA_TOL = {
+    "fp64": np.full(9, 1e-12),
+    "fp32": np.array([1e-5] * 8 + [1e-3]),
+    "mixed": np.array([1e-5] * 8 + [1e-3]),
+}
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
+def test_fma_mode_close_to_oracle(pmhd_lib, oracle, prec):
+    nx = ny = 64
+    Ug, sg = gpu_run(pmhd_lib, prec, nx, ny, 0.05, exact=False)
+    Uo, so = oracle_run(oracle, prec, nx, ny, 0.05)
+    assert sg.steps == so.steps
+    rel = pmhd_lib.relative_l2(interior(Uo), interior(Ug))
+    assert np.all(rel <= FMA_TOL[prec]), rel
