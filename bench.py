@@ -1,0 +1,346 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 2D ideal-MHD + GLM step (pmhd).
+
+Metric: zone-cycles/s (nx * ny * steps / time; one step = both SSPRK2
+stages, the reference's "Mcell-steps/s", src/mhd/mhd2d_glm_gpu.cu:550-554)
+on Orszag-Tang 4096 x 4096, mixed precision (binary32 reconstruction/flux/CFL,
+binary64 state, recovery and update), MUSCL + SSPRK2, HLLD, CFL 0.25,
+alpha 0.18.  The fp64 and fp32 builds are timed beside it at the same size,
+and the relative L2 of mixed against fp64 after the same steps is reported.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 is launched by torchrun, one process per GPU; every rank advances its
+own full-size replica (the single-GPU path has no domain decomposition), the
+timed region is bracketed by a barrier and device synchronisation, and the
+slowest rank's time is used.  `--impl reference` times the reference's own
+serial CPU solver (built from its sources into oracle/_ref/) on the host
+cores instead; only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "precision-study_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "zone-cycles/s at OT 4096²: mixed vs FP64 at stated rel-L2; % HBM roofline"
+UNIT = "zone-cycles/s"
+REF_CPU = os.path.join(ROOT, "oracle", "_ref", "mhd2d_glm_cpu_fp64")
+# Algorithmic HBM bytes per zone-cycle with binary64 storage: stage 1 reads
+# U^n and writes U^1, stage 2 reads U^1 and U^n and writes U^{n+1}:
+# 5 state passes x 9 variables x 8 bytes.  Halo re-reads are excluded.
+B_ALG = {"fp64": 360, "mixed": 360, "fp32": 180}
+# Per stage launch: stage 1 moves 2 passes, stage 2 moves 3; 2.5 on average.
+B_ALG_PER_LAUNCH_CELL = {"fp64": 180, "mixed": 180, "fp32": 90}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.out is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        loaded = [v for v in sm if smax and v > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(precision, n):
+    """DRAM bytes per stage launch from the committed ncu summary, scaled to
+    the n x n grid by cell count; None if no summary exists."""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{precision}.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        txt = f.read()
+    m = re.search(r"dram_bytes_per_cell_per_launch:\s*([0-9.eE+-]+)", txt)
+    return float(m.group(1)) * n * n if m else None
+
+
+def run_reference_cpu(n, instances, t_end=1e-9):
+    """Runs `instances` concurrent copies of the reference CPU solver on an
+    n x n Orszag-Tang grid for one step (t_end below the first dt clips it)
+    and returns (aggregate zone-cycles/s, per-instance walls).  Output files
+    are suppressed by pointing OUTDIR at a path that cannot be created; the
+    solver prints its timing before it tries to write."""
+    if not os.path.exists(REF_CPU):
+        return None, "reference CPU binary missing (run `make -C oracle ref` where the reference is present)"
+    env = dict(os.environ, OUTDIR="/dev/null/pmhd_no_output")
+    args = [REF_CPU, str(n), str(n), repr(t_end), "0.25", "muscl", "hlld", "0.18"]
+    procs = [subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, env=env, text=True)
+             for _ in range(instances)]
+    walls = []
+    for p in procs:
+        out, _ = p.communicate()
+        m = re.search(r"Time loop wall time = ([0-9.eE+-]+) s", out)
+        s = re.search(r"Steps: (\d+)", out)
+        if not m or not s or int(s.group(1)) != 1:
+            return None, "reference CPU run failed"
+        walls.append(float(m.group(1)))
+    return instances * n * n / max(walls), walls
+
+
+def bench_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cores = min(os.cpu_count() or 1, args.ref_instances)
+    n = args.ref_n
+    samples = []
+    for i in range(args.warmup + args.steps):
+        v, info = run_reference_cpu(n, cores)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": info}))
+            return 0
+        if i >= args.warmup:
+            samples.append(v)
+    value = statistics.median(samples)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (Orszag-Tang initial condition)",
+        "ms_per_step": 1e3 * cores * n * n / value,
+        "config": {"workload": f"Orszag-Tang {n}x{n} fp64 one-step samples of the 4096x4096 step, "
+                               "reference serial CPU solver, one process per core",
+                   "nx": n, "ny": n, "instances": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent reference processes x OT {n}x{n} x 1 step per bench step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def time_precision(pmhd, precision, n, warmup, steps, device, sampler=None):
+    """Device-timed throughput of `steps` steps after `warmup` steps."""
+    s = pmhd.Solver(nx=n, ny=n, precision=precision, device=device)
+    s.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
+    if warmup:
+        s.advance(max_steps=warmup)
+    before = s.stats().kernel_launches
+    if sampler is not None:
+        with sampler:
+            st = s.advance(max_steps=steps)
+    else:
+        st = s.advance(max_steps=steps)
+    launches = st.kernel_launches - before
+    return s, st, launches
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the fp64/fp32 lines")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ref-n", type=int, default=1024, help="grid of one reference CPU sample")
+    ap.add_argument("--ref-instances", type=int, default=16, help="max concurrent reference processes")
+    ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return bench_reference(args)
+
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import numpy as np
+    import pmhd
+
+    n, K, W = args.n, args.steps, args.warmup
+    prec = args.precision
+
+    def barrier():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- headline: device-timed throughput of the chosen precision -------
+    sampler = ClockSampler(local)
+    barrier()
+    s, st, launches = time_precision(pmhd, prec, n, W, K, local, sampler)
+    barrier()
+    ms = max_over_ranks(st.device_ms)
+    value = world * n * n * K / (ms / 1e3)
+    clocks = sampler.summary()
+    U_main = s.get_state() if not args.no_compare else None
+    s.close()
+
+    extra = {}
+    if not args.no_compare:
+        for other in ("fp64", "fp32"):
+            if other == prec:
+                continue
+            barrier()
+            so, sto, _ = time_precision(pmhd, other, n, W, K, local)
+            barrier()
+            ms_o = max_over_ranks(sto.device_ms)
+            extra[other] = {"value": world * n * n * K / (ms_o / 1e3), "ms_per_step": ms_o / K}
+            if other == "fp64":
+                U64 = so.get_state()
+                rel = pmhd.relative_l2(U64, U_main)
+                names = ["rho", "mx", "my", "mz", "E", "Bx", "By", "Bz", "psi"]
+                extra["relL2_vs_fp64"] = {k: float(v) for k, v in zip(names, rel)}
+                extra["relL2_vs_fp64_at"] = {"steps": W + K, "t": st.t}
+            so.close()
+        if "fp64" in extra:
+            extra["speedup_vs_fp64"] = value / extra["fp64"]["value"]
+
+    # ---- roofline of the dominant kernel (the stage kernel) -----------------
+    peak, peak_kind = measured_peaks()
+    stage_launches = 2 * K
+    avg_launch_s = (st.device_ms / 1e3) / stage_launches  # includes graph gaps
+    achieved = B_ALG_PER_LAUNCH_CELL[prec] * n * n / avg_launch_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": ncu_traffic(prec, n),
+                "algorithmic_bytes_per_launch": B_ALG_PER_LAUNCH_CELL[prec] * n * n,
+                "avg_launch_ms": avg_launch_s * 1e3, "kernel": "stage_kernel (stage 1 and 2 averaged)"}
+
+    # ---- end to end through the C ABI with pinned host buffers --------------
+    e2e = None
+    if not args.no_e2e:
+        import torch
+        dt = np.float32 if prec == "fp32" else np.float64
+        s2 = pmhd.Solver(nx=n, ny=n, precision=prec, device=local)
+        s2.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
+        host_in = torch.empty((n, n, 9), dtype=torch.float32 if dt == np.float32 else torch.float64,
+                              pin_memory=True).numpy()
+        host_out = torch.empty_like(torch.from_numpy(host_in)).pin_memory().numpy()
+        s2.get_state(out=host_in)
+        s2.advance(max_steps=W)
+        barrier()
+        t0 = time.perf_counter()
+        s2.set_state(host_in)
+        s2.advance(max_steps=K)
+        s2.get_state(out=host_out)
+        t1 = time.perf_counter()
+        barrier()
+        wall = max_over_ranks(t1 - t0)
+        s2.close()
+        nbytes = host_in.nbytes
+        e2e = {"value": world * n * n * K / wall, "unit": UNIT, "h2d_bytes_per_step": nbytes / K,
+               "d2h_bytes_per_step": nbytes / K,
+               "note": "one C-ABI run per timed region: pmhd_set_state from pinned host AoS, "
+                       f"pmhd_advance of {K} steps, pmhd_get_state to pinned host AoS"}
+
+    # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, info = run_reference_cpu(args.cpu_n, 1)
+        if v is not None:
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference mhd2d_glm_cpu fp64 -O2, OT {args.cpu_n}x{args.cpu_n}, 1 step, 1 process"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": info}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "f32 flux/recon/CFL + f64 state/recovery/update", "fp64": "f64",
+                      "fp32": "f32"}[prec],
+            "data": "synthetic (deterministic Orszag-Tang initial condition)",
+            "config": {"workload": f"Orszag-Tang {n}x{n} {prec}, MUSCL+SSPRK2, HLLD eps 1e-4, CFL 0.25, alpha 0.18",
+                       "nx": n, "ny": n, "precision": prec, "exact_ieee": False,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "no flush: each state array is %.2f GB > 126 MB L2" % (
+                           n * n * 9 * (4 if prec == "fp32" else 8) / 1e9)},
+            "roofline": roofline, "gpu_launches": launches, "clocks": clocks, "e2e": e2e,
+            "cpu_baseline": cpu, "steps_run": {"t": st.t, "steps": st.steps},
+        }
+        line.update(extra)
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

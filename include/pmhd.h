@@ -81,8 +81,9 @@ typedef struct {
   int order;                        /* pmhd_order (MUSCL + SSPRK2 or first)    */
   int solver;                       /* pmhd_solver_kind                        */
   int precision;                    /* pmhd_precision                          */
-  int exact;                        /* 1: kernels built without FMA contraction
-                                       (bit-parity mode), 0: FMA enabled      */
+  int exact;                        /* 1: IEEE kernels without FMA contraction
+                                       (bit-parity mode); 0: fast kernels (FMA,
+                                       approximate binary32 div/sqrt)         */
   int bc[4];                        /* x low, x high, y low, y high (pmhd_bc)  */
   int device;                       /* CUDA device ordinal                     */
   int steps_per_graph;              /* steps captured per CUDA graph, 0 = auto */
@@ -123,6 +124,11 @@ int pmhd_destroy(pmhd_solver* s);
  *   BRIO_WU_2D:    params[0] = interface angle in radians (0)
  * gamma, domain and boundary kinds are taken from the handle's config. */
 int pmhd_init_problem(pmhd_solver* s, int problem, const double* params, int nparams);
+
+/* Fills a caller-owned host buffer with problem `problem` for configuration
+ * cfg, without a device: GHOSTED layout, (ny+4)*(nx+4)*9 elements of the
+ * precision's element type.  Same states as pmhd_init_problem uploads. */
+int pmhd_problem_state(const pmhd_config* cfg, int problem, const double* params, int nparams, void* host);
 
 /* Copies a host state into the solver and resets t and the step count.
  * layout INTERIOR: ny*nx*9 values; GHOSTED: (ny+4)*(nx+4)*9 values (the

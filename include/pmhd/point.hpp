@@ -88,11 +88,13 @@ template <class T> PMHD_HD T vsqrt(T a) {
   return std::sqrt(a);
 #endif
 }
+// Finite test in the value's own type (the reference converts to double
+// first; for a float that is the same predicate).
 template <class T> PMHD_HD bool vfinite(T a) {
 #ifdef __CUDA_ARCH__
-  return isfinite((double)a);
+  return isfinite(a);
 #else
-  return std::isfinite((double)a);
+  return std::isfinite(a);
 #endif
 }
 
@@ -270,111 +272,125 @@ PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
 // scale-aware guards; mhdHlldFluxX, mhd_common.hpp:518-654).  Degenerate or
 // non-physical intermediate states fall back to HLL at this interface and
 // return the reason.
+//
+// Same arithmetic as the reference, arranged for a GPU thread: the HLL
+// fallback has a single call site, and only the physical flux of the side
+// the final formula uses is evaluated (the reference evaluates both up
+// front; the unused one never reaches F).  The side test `sm >= 0` selects
+// the same branch as the reference's chain sLs >= 0 / sm >= 0 / sRs >= 0
+// because sLs <= sm <= sRs, and NaN reaches the same last branch.
 template <class T, int AX>
 PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
   using D = Dir<AX>;
-  T WL[NV8], WR[NV8], FL[NV8], FR[NV8];
+  T WL[NV8], WR[NV8];
   cons_to_prim<T, AX>(UL, WL, ph);
   cons_to_prim<T, AX>(UR, WR, ph);
-  phys_flux<T, AX>(WL, UL[EN], FL);
-  phys_flux<T, AX>(WR, UR[EN], FR);
   const T cfL = fast_speed<T, AX>(WL, ph);
   const T cfR = fast_speed<T, AX>(WR, ph);
   const T sL = vmin(WL[D::vn] - cfL, WR[D::vn] - cfR);
   const T sR = vmax(WL[D::vn] + cfL, WR[D::vn] + cfR);
   if (sL >= (T)0.0) {
-#pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FL[k];
+    phys_flux<T, AX>(WL, UL[EN], F);
     return HLLD_OK;
   }
   if (sR <= (T)0.0) {
-#pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FR[k];
+    phys_flux<T, AX>(WR, UR[EN], F);
     return HLLD_OK;
   }
-  const T rhoL = vmax(WL[RHO], rho_floor<T>());
-  const T rhoR = vmax(WR[RHO], rho_floor<T>());
-  const T vnL = WL[D::vn], vnR = WR[D::vn];
-  const T bn = (T)0.5 * (WL[D::bn] + WR[D::bn]);
-  const T b2L = bn * bn + WL[D::bt1] * WL[D::bt1] + WL[D::bt2] * WL[D::bt2];
-  const T b2R = bn * bn + WR[D::bt1] * WR[D::bt1] + WR[D::bt2] * WR[D::bt2];
-  const T ptL = vmax(WL[EN], p_floor<T>()) + (T)0.5 * b2L;
-  const T ptR = vmax(WR[EN], p_floor<T>()) + (T)0.5 * b2R;
-  const T denom_sm = rhoR * (sR - vnR) - rhoL * (sL - vnL);
-  const T denom_sm_scale = vabs(rhoR * (sR - vnR)) + vabs(rhoL * (sL - vnL));
-  const T b_scale = vsqrt(vmax(b2L, b2R));
-  if (hlld_small(denom_sm, denom_sm_scale, ph) || hlld_small(bn, b_scale, ph)) {
-    hll_flux<T, AX>(UL, UR, F, ph);
-    return HLLD_FALLBACK_DEGENERATE;
-  }
-  const T sm = (rhoR * vnR * (sR - vnR) - rhoL * vnL * (sL - vnL) + ptL - ptR) / denom_sm;
-  const T ptsL = ptL + rhoL * (sL - vnL) * (sm - vnL);
-  const T ptsR = ptR + rhoR * (sR - vnR) * (sm - vnR);
-  const T pts = (T)0.5 * (ptsL + ptsR);
-  T ULs[NV8], URs[NV8];
-  const int stL = hlld_star<T, AX>(UL, WL, sL, sm, pts, bn, ULs, ph);
-  const int stR = hlld_star<T, AX>(UR, WR, sR, sm, pts, bn, URs, ph);
-  if (stL != HLLD_OK || stR != HLLD_OK) {
-    hll_flux<T, AX>(UL, UR, F, ph);
-    return (stL != HLLD_OK) ? stL : stR;
-  }
-  const T sqL = vsqrt(vmax(ULs[RHO], rho_floor<T>()));
-  const T sqR = vsqrt(vmax(URs[RHO], rho_floor<T>()));
-  const T sgn = (bn < (T)0.0) ? (T)-1.0 : (T)1.0;
-  const T sLs = sm - vabs(bn) / sqL;
-  const T sRs = sm + vabs(bn) / sqR;
-  const T den = sqL + sqR;
-  if (den <= (T)0.0) {
-    hll_flux<T, AX>(UL, UR, F, ph);
-    return HLLD_FALLBACK_DEGENERATE;
-  }
-  const T vt1Ls = ULs[D::vt1] / ULs[RHO], vt2Ls = ULs[D::vt2] / ULs[RHO];
-  const T bt1Ls = ULs[D::bt1], bt2Ls = ULs[D::bt2];
-  const T vt1Rs = URs[D::vt1] / URs[RHO], vt2Rs = URs[D::vt2] / URs[RHO];
-  const T bt1Rs = URs[D::bt1], bt2Rs = URs[D::bt2];
-  const T vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) / den;
-  const T vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) / den;
-  const T bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) / den;
-  const T bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) / den;
-  // Double-star states differ from the star states only in the tangential
-  // slots and the energy.
-  T ULD[NV8], URD[NV8];
+  int status = HLLD_OK;
+  do {
+    const T rhoL = vmax(WL[RHO], rho_floor<T>());
+    const T rhoR = vmax(WR[RHO], rho_floor<T>());
+    const T vnL = WL[D::vn], vnR = WR[D::vn];
+    const T bn = (T)0.5 * (WL[D::bn] + WR[D::bn]);
+    const T b2L = bn * bn + WL[D::bt1] * WL[D::bt1] + WL[D::bt2] * WL[D::bt2];
+    const T b2R = bn * bn + WR[D::bt1] * WR[D::bt1] + WR[D::bt2] * WR[D::bt2];
+    const T ptL = vmax(WL[EN], p_floor<T>()) + (T)0.5 * b2L;
+    const T ptR = vmax(WR[EN], p_floor<T>()) + (T)0.5 * b2R;
+    const T denom_sm = rhoR * (sR - vnR) - rhoL * (sL - vnL);
+    const T denom_sm_scale = vabs(rhoR * (sR - vnR)) + vabs(rhoL * (sL - vnL));
+    const T b_scale = vsqrt(vmax(b2L, b2R));
+    if (hlld_small(denom_sm, denom_sm_scale, ph) || hlld_small(bn, b_scale, ph)) {
+      status = HLLD_FALLBACK_DEGENERATE;
+      break;
+    }
+    const T sm = (rhoR * vnR * (sR - vnR) - rhoL * vnL * (sL - vnL) + ptL - ptR) / denom_sm;
+    const T ptsL = ptL + rhoL * (sL - vnL) * (sm - vnL);
+    const T ptsR = ptR + rhoR * (sR - vnR) * (sm - vnR);
+    const T pts = (T)0.5 * (ptsL + ptsR);
+    T ULs[NV8], URs[NV8];
+    const int stL = hlld_star<T, AX>(UL, WL, sL, sm, pts, bn, ULs, ph);
+    const int stR = hlld_star<T, AX>(UR, WR, sR, sm, pts, bn, URs, ph);
+    if (stL != HLLD_OK || stR != HLLD_OK) {
+      status = (stL != HLLD_OK) ? stL : stR;
+      break;
+    }
+    const T sqL = vsqrt(vmax(ULs[RHO], rho_floor<T>()));
+    const T sqR = vsqrt(vmax(URs[RHO], rho_floor<T>()));
+    const T sgn = (bn < (T)0.0) ? (T)-1.0 : (T)1.0;
+    const T sLs = sm - vabs(bn) / sqL;
+    const T sRs = sm + vabs(bn) / sqR;
+    const T den = sqL + sqR;
+    if (den <= (T)0.0) {
+      status = HLLD_FALLBACK_DEGENERATE;
+      break;
+    }
+    const T vt1Ls = ULs[D::vt1] / ULs[RHO], vt2Ls = ULs[D::vt2] / ULs[RHO];
+    const T bt1Ls = ULs[D::bt1], bt2Ls = ULs[D::bt2];
+    const T vt1Rs = URs[D::vt1] / URs[RHO], vt2Rs = URs[D::vt2] / URs[RHO];
+    const T bt1Rs = URs[D::bt1], bt2Rs = URs[D::bt2];
+    const T vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) / den;
+    const T vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) / den;
+    const T bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) / den;
+    const T bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) / den;
+    const T vbD = sm * bn + vt1D * bt1D + vt2D * bt2D;
+    const T vbLs = sm * bn + vt1Ls * bt1Ls + vt2Ls * bt2Ls;
+    const T vbRs = sm * bn + vt1Rs * bt1Rs + vt2Rs * bt2Rs;
+    // Double-star states differ from the star states only in the tangential
+    // slots and the energy.
+    T ULD[NV8], URD[NV8];
 #pragma unroll
-  for (int k = 0; k < NV8; k++) {
-    ULD[k] = ULs[k];
-    URD[k] = URs[k];
-  }
-  ULD[D::vt1] = ULD[RHO] * vt1D;
-  ULD[D::vt2] = ULD[RHO] * vt2D;
-  ULD[D::bt1] = bt1D;
-  ULD[D::bt2] = bt2D;
-  URD[D::vt1] = URD[RHO] * vt1D;
-  URD[D::vt2] = URD[RHO] * vt2D;
-  URD[D::bt1] = bt1D;
-  URD[D::bt2] = bt2D;
-  const T vbD = sm * bn + vt1D * bt1D + vt2D * bt2D;
-  const T vbLs = sm * bn + vt1Ls * bt1Ls + vt2Ls * bt2Ls;
-  const T vbRs = sm * bn + vt1Rs * bt1Rs + vt2Rs * bt2Rs;
-  ULD[EN] = ULs[EN] - sgn * sqL * (vbLs - vbD);
-  URD[EN] = URs[EN] + sgn * sqR * (vbRs - vbD);
-  if (!positive_state<T, AX>(ULD, ph) || !positive_state<T, AX>(URD, ph)) {
-    hll_flux<T, AX>(UL, UR, F, ph);
-    return HLLD_FALLBACK_NONPHYSICAL;
-  }
-  if (sLs >= (T)0.0) {
+    for (int k = 0; k < NV8; k++) {
+      ULD[k] = ULs[k];
+      URD[k] = URs[k];
+    }
+    ULD[D::vt1] = ULD[RHO] * vt1D;
+    ULD[D::vt2] = ULD[RHO] * vt2D;
+    ULD[D::bt1] = bt1D;
+    ULD[D::bt2] = bt2D;
+    URD[D::vt1] = URD[RHO] * vt1D;
+    URD[D::vt2] = URD[RHO] * vt2D;
+    URD[D::bt1] = bt1D;
+    URD[D::bt2] = bt2D;
+    ULD[EN] = ULs[EN] - sgn * sqL * (vbLs - vbD);
+    URD[EN] = URs[EN] + sgn * sqR * (vbRs - vbD);
+    if (!positive_state<T, AX>(ULD, ph) || !positive_state<T, AX>(URD, ph)) {
+      status = HLLD_FALLBACK_NONPHYSICAL;
+      break;
+    }
+    if (sm >= (T)0.0) {
+      phys_flux<T, AX>(WL, UL[EN], F);
+      if (sLs >= (T)0.0) {
 #pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FL[k] + sL * (ULs[k] - UL[k]);
-  } else if (sm >= (T)0.0) {
+        for (int k = 0; k < NV8; k++) F[k] = F[k] + sL * (ULs[k] - UL[k]);
+      } else {
 #pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FL[k] + sL * (ULs[k] - UL[k]) + sLs * (ULD[k] - ULs[k]);
-  } else if (sRs >= (T)0.0) {
+        for (int k = 0; k < NV8; k++) F[k] = F[k] + sL * (ULs[k] - UL[k]) + sLs * (ULD[k] - ULs[k]);
+      }
+    } else {
+      phys_flux<T, AX>(WR, UR[EN], F);
+      if (sRs >= (T)0.0) {
 #pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FR[k] + sR * (URs[k] - UR[k]) + sRs * (URD[k] - URs[k]);
-  } else {
+        for (int k = 0; k < NV8; k++) F[k] = F[k] + sR * (URs[k] - UR[k]) + sRs * (URD[k] - URs[k]);
+      } else {
 #pragma unroll
-    for (int k = 0; k < NV8; k++) F[k] = FR[k] + sR * (URs[k] - UR[k]);
-  }
-  return HLLD_OK;
+        for (int k = 0; k < NV8; k++) F[k] = F[k] + sR * (URs[k] - UR[k]);
+      }
+    }
+    return HLLD_OK;
+  } while (false);
+  hll_flux<T, AX>(UL, UR, F, ph);
+  return status;
 }
 
 // Mixed-GLM interface flux along AX (mhdGlmNormalState + mhdGlmFluxX/Y,

@@ -263,6 +263,11 @@ void OF(or_point_recon)(const OT Pm[9], const OT P0[9], const OT Pp[9], OT Pl[9]
   OF(or_recon)(Pm, P0, Pp, Pl, Pr);
 }
 void OF(or_fill_ghosts)(const or_config* cfg, OT* U) { OF(or_apply_bc)(U, cfg->nx, cfg->ny, cfg->bc); }
+OT OF(or_point_minmod)(OT a, OT b) { return OF(or_minmod)(a, b); }
+int OF(or_point_positive)(const OT U[8], double gamma) {
+  OF(or_phys) ph = {(OT)gamma, (OT)0};
+  return OF(or_positive)(U, &ph);
+}
 
 #undef OF
 #undef OR_CAT

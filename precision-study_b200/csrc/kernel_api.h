@@ -1,9 +1,12 @@
 // kernel_api.h -- host-side interface of the pmhd CUDA kernels.
 //
-// The kernels are compiled twice from the same source: once with
-// floating-point contraction disabled (-fmad=false, table "exact", the
-// bit-parity mode against the reference CPU build) and once with it enabled
-// (table "fma", the performance mode).  solver.cpp picks a table per handle.
+// The kernels are compiled twice from the same source: once with IEEE
+// arithmetic and floating-point contraction disabled (-fmad=false, table
+// "exact", the bit-parity mode against the reference CPU build) and once for
+// speed (table "fast": FMA contraction, and binary32 division and square
+// root with the hardware's approximate instructions, at most 2 ulp; binary64
+// arithmetic stays IEEE apart from contraction).  solver.cpp picks a table
+// per handle.
 #ifndef PMHD_KERNEL_API_H
 #define PMHD_KERNEL_API_H
 
@@ -48,7 +51,7 @@ struct KernelTable {
 };
 
 const KernelTable& kernel_table_exact();
-const KernelTable& kernel_table_fma();
+const KernelTable& kernel_table_fast();
 
 }  // namespace pmhd
 

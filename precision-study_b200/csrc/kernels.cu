@@ -1,7 +1,8 @@
 // kernels.cu -- instantiates the pmhd kernels for every precision policy and
 // exposes them through a KernelTable.  Built twice by the Makefile:
-//   -DPMHD_KNS=exact -fmad=false  -> kernel_table_exact()
-//   -DPMHD_KNS=fma   -fmad=true   -> kernel_table_fma()
+//   -DPMHD_KNS=exact -fmad=false                  -> kernel_table_exact()
+//   -DPMHD_KNS=fast  -fmad=true -prec-div=false -prec-sqrt=false
+//                                                 -> kernel_table_fast()
 #include "stage_kernels.cuh"
 
 namespace pmhd {
@@ -59,7 +60,7 @@ static cudaError_t launch_stage(int precision, int hlld, int stage, const void* 
 }
 
 static int grid_for(long long n) {
-  long long b = (n + NT - 1) / NT;
+  long long b = (n + NTA - 1) / NTA;
   if (b > 148 * 64) b = 148 * 64;
   return (int)(b < 1 ? 1 : b);
 }
@@ -69,13 +70,13 @@ static cudaError_t launch_speed(int precision, const void* u, long long plane, i
   const int g = grid_for((long long)nx * ny);
   switch (precision) {
     case PREC_FP64:
-      speed_kernel<PolF64><<<g, NT, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, gamma, ctrl, slot);
+      speed_kernel<PolF64><<<g, NTA, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, gamma, ctrl, slot);
       break;
     case PREC_FP32:
-      speed_kernel<PolF32><<<g, NT, 0, s>>>(static_cast<const float*>(u), plane, nx, ny, pitch, gamma, ctrl, slot);
+      speed_kernel<PolF32><<<g, NTA, 0, s>>>(static_cast<const float*>(u), plane, nx, ny, pitch, gamma, ctrl, slot);
       break;
     case PREC_MIXED:
-      speed_kernel<PolMixed><<<g, NT, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, gamma, ctrl,
+      speed_kernel<PolMixed><<<g, NTA, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, gamma, ctrl,
                                               slot);
       break;
     default: return cudaErrorInvalidValue;
@@ -87,10 +88,10 @@ static cudaError_t launch_aos_to_soa(int precision, const void* aos, int layout,
                                      int ny, int pitch, const int bc[4], cudaStream_t s) {
   const int g = grid_for((long long)nx * ny);
   if (precision == PREC_FP32)
-    aos_to_soa_kernel<float><<<g, NT, 0, s>>>(static_cast<const float*>(aos), layout, static_cast<float*>(u), plane,
+    aos_to_soa_kernel<float><<<g, NTA, 0, s>>>(static_cast<const float*>(aos), layout, static_cast<float*>(u), plane,
                                               nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
   else
-    aos_to_soa_kernel<double><<<g, NT, 0, s>>>(static_cast<const double*>(aos), layout, static_cast<double*>(u),
+    aos_to_soa_kernel<double><<<g, NTA, 0, s>>>(static_cast<const double*>(aos), layout, static_cast<double*>(u),
                                                plane, nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
   return cudaGetLastError();
 }
@@ -100,10 +101,10 @@ static cudaError_t launch_soa_to_aos(int precision, const void* u, long long pla
   const long long n = layout == 0 ? (long long)nx * ny : (long long)(nx + 4) * (ny + 4);
   const int g = grid_for(n);
   if (precision == PREC_FP32)
-    soa_to_aos_kernel<float><<<g, NT, 0, s>>>(static_cast<const float*>(u), plane, nx, ny, pitch, layout,
+    soa_to_aos_kernel<float><<<g, NTA, 0, s>>>(static_cast<const float*>(u), plane, nx, ny, pitch, layout,
                                               static_cast<float*>(aos));
   else
-    soa_to_aos_kernel<double><<<g, NT, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, layout,
+    soa_to_aos_kernel<double><<<g, NTA, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, layout,
                                                static_cast<double*>(aos));
   return cudaGetLastError();
 }

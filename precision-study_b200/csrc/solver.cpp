@@ -278,7 +278,7 @@ int pmhd_create(const pmhd_config* cfg, pmhd_solver** out) {
   if (!s) return PMHD_ERR_NOMEM;
   s->cfg = *cfg;
   if (s->cfg.steps_per_graph == 0) s->cfg.steps_per_graph = 32;
-  s->kt = cfg->exact ? &kernel_table_exact() : &kernel_table_fma();
+  s->kt = cfg->exact ? &kernel_table_exact() : &kernel_table_fast();
   {
     std::lock_guard<std::mutex> lk(g_init_mu);
     const int dev = cfg->device & 63, which = cfg->exact ? 1 : 0;
@@ -375,17 +375,40 @@ int pmhd_set_time(pmhd_solver* s, double t, long long steps) {
   return PMHD_OK;
 }
 
-int pmhd_init_problem(pmhd_solver* s, int problem, const double* params, int nparams) {
-  if (!s || nparams < 0) return PMHD_ERR_ARG;
-  const ProblemGrid g = grid_of(s);
-  if (is_fp32(s)) {
+int pmhd_problem_state(const pmhd_config* cfg, int problem, const double* params, int nparams, void* host) {
+  if (!host || nparams < 0 || check_args(cfg) != PMHD_OK) return PMHD_ERR_ARG;
+  ProblemGrid g;
+  g.nx = cfg->nx;
+  g.ny = cfg->ny;
+  g.x_min = cfg->x_min;
+  g.x_max = cfg->x_max;
+  g.y_min = cfg->y_min;
+  g.y_max = cfg->y_max;
+  g.gamma = cfg->gamma;
+  const size_t n = (size_t)(cfg->nx + 4) * (cfg->ny + 4) * 9;
+  if (cfg->precision == PMHD_FP32) {
     std::vector<float> U;
     if (!init_problem_host<float>(g, problem, params, nparams, U)) return PMHD_ERR_ARG;
-    return pmhd_set_state(s, U.data(), PMHD_LAYOUT_GHOSTED);
+    std::memcpy(host, U.data(), n * sizeof(float));
+  } else {
+    std::vector<double> U;
+    if (!init_problem_host<double>(g, problem, params, nparams, U)) return PMHD_ERR_ARG;
+    std::memcpy(host, U.data(), n * sizeof(double));
   }
-  std::vector<double> U;
-  if (!init_problem_host<double>(g, problem, params, nparams, U)) return PMHD_ERR_ARG;
-  return pmhd_set_state(s, U.data(), PMHD_LAYOUT_GHOSTED);
+  return PMHD_OK;
+}
+
+int pmhd_init_problem(pmhd_solver* s, int problem, const double* params, int nparams) {
+  if (!s || nparams < 0) return PMHD_ERR_ARG;
+  const size_t n = (size_t)(s->cfg.nx + 4) * (s->cfg.ny + 4) * 9;
+  if (is_fp32(s)) {
+    std::vector<float> U(n);
+    int rc = pmhd_problem_state(&s->cfg, problem, params, nparams, U.data());
+    return rc != PMHD_OK ? rc : pmhd_set_state(s, U.data(), PMHD_LAYOUT_GHOSTED);
+  }
+  std::vector<double> U(n);
+  int rc = pmhd_problem_state(&s->cfg, problem, params, nparams, U.data());
+  return rc != PMHD_OK ? rc : pmhd_set_state(s, U.data(), PMHD_LAYOUT_GHOSTED);
 }
 
 int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* stats) {

@@ -40,7 +40,7 @@
 #include "pmhd/point.hpp"
 
 #ifndef PMHD_KNS
-#error "PMHD_KNS (kernel namespace: exact or fma) must be defined"
+#error "PMHD_KNS (kernel namespace: exact or fast) must be defined"
 #endif
 
 namespace pmhd {
@@ -68,12 +68,14 @@ struct PolMixed {
 constexpr int TX = 32, TY = 8;            // output tile
 constexpr int HX = TX + 4, HY = TY + 4;   // tile with halo
 constexpr int TC = HX * HY;               // cells per loaded tile
-constexpr int NT = 256;                   // threads per CTA (one per output cell)
+constexpr int NCELL = TX * TY;            // output cells per tile
+constexpr int NW = NCELL / 32 + 1;        // warps per CTA: one per tile row + one
+constexpr int NT = NW * 32;               // threads per stage CTA (288)
+constexpr int NTA = 256;                  // threads per CTA of the auxiliary kernels
 constexpr int FXN = TY * (TX + 1);        // x-interfaces per tile
 constexpr int GYN = (TY + 1) * TX;        // y-interfaces per tile
-constexpr int XW = (FXN + 31) / 32;       // warps of x-interface work
-constexpr int YW = (GYN + 31) / 32;       // warps of y-interface work
 constexpr uint32_t kWaitIters = 1u << 22; // bound on mbarrier polls
+static_assert(TX == 32, "one warp per tile row");
 
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 
@@ -174,9 +176,13 @@ __device__ __forceinline__ int face_flux(const typename Pol::S* sU, const typena
   return glm_flux<R, AX>(UL, UR, ch, HLLD, F, ph);
 }
 
+// Resident CTAs per SM the register allocation is sized for: two for the
+// binary32-flux policies; one for binary64, whose HLLD needs more registers
+// than two resident CTAs leave per thread (spilling costs more than the lost
+// occupancy).
 template <class Pol>
 struct StageMinBlocks {
-  static constexpr int value = (sizeof(typename Pol::S) == 8 && sizeof(typename Pol::R) == 8) ? 2 : 3;
+  static constexpr int value = sizeof(typename Pol::R) == 8 ? 1 : 2;
 };
 
 template <class Pol, int STAGE, bool HLLD>
@@ -191,8 +197,8 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
   R* sFx = reinterpret_cast<R*>(smem_raw + Smem<Pol>::fx_off);
   R* sGy = reinterpret_cast<R*>(smem_raw + Smem<Pol>::gy_off);
   __shared__ __align__(8) uint64_t bar;
-  __shared__ unsigned long long red_speed[NT / 32];
-  __shared__ unsigned red_deg[NT / 32], red_np[NT / 32];
+  __shared__ unsigned long long red_speed[NW];
+  __shared__ unsigned red_deg[NW], red_np[NW];
 
   const int tid = threadIdx.x;
   const bool leader = (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0);
@@ -262,49 +268,51 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
   }
 
   // ---- 3. interface fluxes --------------------------------------------------
+  // Warps 0..TY-1 own one tile row each: lane tx computes the x-interface to
+  // the right of cell (tx, ty), then the y-interface above it.  The last warp
+  // computes the tile's bottom row of y-interfaces, then its left column of
+  // x-interfaces.  Every warp runs two rounds of one direction each, so no
+  // warp lags at the barrier and no warp mixes the two code paths.
   const int warp = tid >> 5, lane = tid & 31;
   unsigned n_deg = 0, n_np = 0;
-  for (int vw = warp; vw < XW + YW; vw += NT / 32) {
+  auto x_face = [&](int fx, int fy) {
+    const int gi = i0 + fx;  // interface between cells gi-1 and gi
+    if (gi > a.nx || j0 + fy >= a.ny) return;
     R F[NVAR];
-    if (vw < XW) {
-      const int item = vw * 32 + lane;
-      if (item < FXN) {
-        const int fx = item % (TX + 1), fy = item / (TX + 1);
-        const int gi = i0 + fx;  // interface between cells gi-1 and gi
-        if (gi <= a.nx && j0 + fy < a.ny) {
-          const int st = face_flux<Pol, 0, HLLD>(sU, sP, (fy + 2) * HX + fx, 1, a.muscl, ch, phR, F);
+    const int st = face_flux<Pol, 0, HLLD>(sU, sP, (fy + 2) * HX + fx, 1, a.muscl, ch, phR, F);
 #pragma unroll
-          for (int k = 0; k < NVAR; k++) sFx[k * FXN + item] = F[k];
-          if (HLLD && (fx >= 1 || i0 == 0)) {
-            n_deg += (st == HLLD_FALLBACK_DEGENERATE);
-            n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
-          }
-        }
-      }
-    } else {
-      const int item = (vw - XW) * 32 + lane;
-      if (item < GYN) {
-        const int fx = item % TX, fy = item / TX;
-        const int gj = j0 + fy;  // interface between rows gj-1 and gj
-        if (gj <= a.ny && i0 + fx < a.nx) {
-          const int st = face_flux<Pol, 1, HLLD>(sU, sP, fy * HX + fx + 2, HX, a.muscl, ch, phR, F);
-#pragma unroll
-          for (int k = 0; k < NVAR; k++) sGy[k * GYN + item] = F[k];
-          if (HLLD && (fy >= 1 || j0 == 0)) {
-            n_deg += (st == HLLD_FALLBACK_DEGENERATE);
-            n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
-          }
-        }
-      }
+    for (int k = 0; k < NVAR; k++) sFx[k * FXN + fy * (TX + 1) + fx] = F[k];
+    if (HLLD && (fx >= 1 || i0 == 0)) {
+      n_deg += (st == HLLD_FALLBACK_DEGENERATE);
+      n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
     }
+  };
+  auto y_face = [&](int fx, int fy) {
+    const int gj = j0 + fy;  // interface between rows gj-1 and gj
+    if (gj > a.ny || i0 + fx >= a.nx) return;
+    R F[NVAR];
+    const int st = face_flux<Pol, 1, HLLD>(sU, sP, fy * HX + fx + 2, HX, a.muscl, ch, phR, F);
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) sGy[k * GYN + fy * TX + fx] = F[k];
+    if (HLLD && (fy >= 1 || j0 == 0)) {
+      n_deg += (st == HLLD_FALLBACK_DEGENERATE);
+      n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
+    }
+  };
+  if (warp < TY) {
+    x_face(lane + 1, warp);
+    y_face(lane, warp + 1);
+  } else {
+    y_face(lane, 0);
+    if (lane < TY) x_face(0, lane);
   }
   __syncthreads();
 
   // ---- 4. divergence, update, checks, store, next-step speed ---------------
-  const int tx = tid % TX, ty = tid / TX;
+  const int tx = lane, ty = warp;
   const int gi = i0 + tx, gj = j0 + ty;
   unsigned long long sp_bits = 0;
-  if (gi < a.nx && gj < a.ny) {
+  if (warp < TY && gi < a.nx && gj < a.ny) {
     const int lc = (ty + 2) * HX + (tx + 2);
     const size_t gidx = (size_t)(gj + GHOST) * a.pitch + (gi + GHOST);
     S Un[NVAR];
@@ -343,15 +351,17 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
         }
       }
     }
-    if (!state_usable<S>(Un, phS)) {
+    // stateIsUsable (mhd2d_glm_gpu.cu:74-79); its recovery doubles as the
+    // recovery of the next step's CFL speed (speedKernel, :171-195).
+    S P9[NVAR];
+    state_to_prim9<S>(Un, P9, phS);
+    if (!(Un[RHO] > rho_floor<S>()) || !prim9_usable<S>(P9)) {
       atomicMin(STAGE == 1 ? &c->bad1 : &c->bad2, gj * a.nx + gi);
       c->bad_step = step;
     }
     store_cell<S>(static_cast<S*>(a.u_out), a.plane, a.pitch, gi, gj, a.nx, a.ny, a.bc, Un);
     if (STAGE == 2) {
-      S P9[NVAR];
       R Pr[NVAR];
-      state_to_prim9<S>(Un, P9, phS);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
       sp_bits = speed_bits((double)cell_speed<R>(Pr, phR));
@@ -375,7 +385,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
     if (HLLD) {
       unsigned d = 0, np = 0;
 #pragma unroll
-      for (int w = 0; w < NT / 32; w++) {
+      for (int w = 0; w < NW; w++) {
         d += red_deg[w];
         np += red_np[w];
       }
@@ -385,7 +395,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
     if (STAGE == 2) {
       unsigned long long m = 0;
 #pragma unroll
-      for (int w = 0; w < NT / 32; w++) m = red_speed[w] > m ? red_speed[w] : m;
+      for (int w = 0; w < NW; w++) m = red_speed[w] > m ? red_speed[w] : m;
       if (m) atomicMax(&c->chbits[p ^ 1], m);
     }
   }
@@ -404,7 +414,7 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
 
 // ---- initial CFL speed: max over interior cells into chbits[slot] ----------
 template <class Pol>
-__global__ void __launch_bounds__(NT) speed_kernel(const typename Pol::S* __restrict__ u, long long plane, int nx,
+__global__ void __launch_bounds__(NTA) speed_kernel(const typename Pol::S* __restrict__ u, long long plane, int nx,
                                                    int ny, int pitch, double gamma, Ctrl* c, int slot) {
   using S = typename Pol::S;
   using R = typename Pol::R;
@@ -412,7 +422,7 @@ __global__ void __launch_bounds__(NT) speed_kernel(const typename Pol::S* __rest
   const Phys<R> phR = Phys<R>::make(gamma, 0.0);
   unsigned long long m = 0;
   const long long n = (long long)nx * ny;
-  for (long long q = blockIdx.x * (long long)NT + threadIdx.x; q < n; q += (long long)gridDim.x * NT) {
+  for (long long q = blockIdx.x * (long long)NTA + threadIdx.x; q < n; q += (long long)gridDim.x * NTA) {
     const int i = (int)(q % nx), j = (int)(q / nx);
     const size_t g = (size_t)(j + GHOST) * pitch + (i + GHOST);
     S U9[NVAR], P9[NVAR];
@@ -425,12 +435,12 @@ __global__ void __launch_bounds__(NT) speed_kernel(const typename Pol::S* __rest
     const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, phR));
     m = b > m ? b : m;
   }
-  __shared__ unsigned long long red[NT / 32];
+  __shared__ unsigned long long red[NTA / 32];
   m = warp_max_u64(m);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < NT / 32; w++) m = red[w] > m ? red[w] : m;
+    for (int w = 1; w < NTA / 32; w++) m = red[w] > m ? red[w] : m;
     if (m) atomicMax(&c->chbits[slot], m);
   }
 }
@@ -440,12 +450,12 @@ __global__ void __launch_bounds__(NT) speed_kernel(const typename Pol::S* __rest
 // ghosted array, [(ny+4)][(nx+4)][9] (ghost values are rebuilt from the
 // boundary conditions on input).
 template <class S>
-__global__ void __launch_bounds__(NT) aos_to_soa_kernel(const S* __restrict__ aos, int layout, S* u, long long plane,
+__global__ void __launch_bounds__(NTA) aos_to_soa_kernel(const S* __restrict__ aos, int layout, S* u, long long plane,
                                                         int nx, int ny, int pitch, int bc0, int bc1, int bc2,
                                                         int bc3) {
   const int bc[4] = {bc0, bc1, bc2, bc3};
   const long long n = (long long)nx * ny;
-  for (long long q = blockIdx.x * (long long)NT + threadIdx.x; q < n; q += (long long)gridDim.x * NT) {
+  for (long long q = blockIdx.x * (long long)NTA + threadIdx.x; q < n; q += (long long)gridDim.x * NTA) {
     const int i = (int)(q % nx), j = (int)(q / nx);
     const size_t src = layout == 0 ? (size_t)q * NVAR : ((size_t)(j + GHOST) * (nx + 4) + (i + GHOST)) * NVAR;
     S v[NVAR];
@@ -456,11 +466,11 @@ __global__ void __launch_bounds__(NT) aos_to_soa_kernel(const S* __restrict__ ao
 }
 
 template <class S>
-__global__ void __launch_bounds__(NT) soa_to_aos_kernel(const S* __restrict__ u, long long plane, int nx, int ny,
+__global__ void __launch_bounds__(NTA) soa_to_aos_kernel(const S* __restrict__ u, long long plane, int nx, int ny,
                                                         int pitch, int layout, S* __restrict__ aos) {
   const int wx = layout == 0 ? nx : nx + 4, wy = layout == 0 ? ny : ny + 4, off = layout == 0 ? GHOST : 0;
   const long long n = (long long)wx * wy;
-  for (long long q = blockIdx.x * (long long)NT + threadIdx.x; q < n; q += (long long)gridDim.x * NT) {
+  for (long long q = blockIdx.x * (long long)NTA + threadIdx.x; q < n; q += (long long)gridDim.x * NTA) {
     const int i = (int)(q % wx), j = (int)(q / wx);
     const size_t g = (size_t)(j + off) * pitch + (i + off);
 #pragma unroll

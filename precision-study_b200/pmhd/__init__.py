@@ -18,7 +18,7 @@ import os
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libpmhd.so")
+LIB_PATH = os.environ.get("PMHD_LIB") or os.path.join(PKG_DIR, "libpmhd.so")
 CLI_PATH = os.path.join(PKG_DIR, "bin", "mhd2d_glm_gpu")
 
 OK, ERR_ARG, ERR_RATE, ERR_STAGE1, ERR_STAGE2, ERR_IO, ERR_CUDA = 0, 1, 2, 3, 4, 5, 9
@@ -37,7 +37,7 @@ EXPORTS = (
     "pmhd_config_default", "pmhd_create", "pmhd_destroy", "pmhd_init_problem",
     "pmhd_set_state", "pmhd_get_state", "pmhd_set_time", "pmhd_advance",
     "pmhd_get_stats", "pmhd_diagnostics", "pmhd_write_dat", "pmhd_dat_filename",
-    "pmhd_strerror", "pmhd_get_config",
+    "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state",
 )
 
 
@@ -103,6 +103,7 @@ def load():
         "pmhd_dat_filename": ([vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t], i),
         "pmhd_strerror": ([i], ctypes.c_char_p),
         "pmhd_get_config": ([vp, P(Config)], i),
+        "pmhd_problem_state": ([P(Config), i, P(d), i, vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -122,6 +123,38 @@ def default_config():
     return c
 
 
+def problem_state(problem, params=None, **cfg_kwargs):
+    """Host-only initial state (ghosted AoS) of `problem` for the
+    configuration Solver(**cfg_kwargs) would use; needs no GPU."""
+    c = make_config(**cfg_kwargs)
+    dt = np.float32 if c.precision == FP32 else np.float64
+    U = np.empty((c.ny + 4, c.nx + 4, 9), dtype=dt)
+    arr, n = None, 0
+    if params is not None:
+        n = len(params)
+        arr = (ctypes.c_double * n)(*params)
+    _check(load().pmhd_problem_state(ctypes.byref(c), problem, arr, n, U.ctypes.data), "pmhd_problem_state")
+    return U
+
+
+def make_config(nx=128, ny=128, precision="fp64", exact=False, order="muscl", solver="hlld", cfl=0.25,
+                alpha=0.18, gamma=5.0 / 3.0, hlld_tol=1e-4, domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0),
+                device=0, steps_per_graph=0):
+    c = default_config()
+    c.nx, c.ny = nx, ny
+    c.x_min, c.x_max, c.y_min, c.y_max = domain
+    c.gamma, c.hlld_tol, c.cfl, c.alpha = gamma, hlld_tol, cfl, alpha
+    c.order = ORDER_MUSCL if order == "muscl" else ORDER_FIRST
+    c.solver = SOLVER_HLLD if solver == "hlld" else SOLVER_HLL
+    c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    c.exact = int(bool(exact))
+    for k in range(4):
+        c.bc[k] = bc[k]
+    c.device = device
+    c.steps_per_graph = steps_per_graph
+    return c
+
+
 def _check(status, where):
     if status != OK:
         raise PmhdError(status, where)
@@ -134,18 +167,8 @@ class Solver:
                  solver="hlld", cfl=0.25, alpha=0.18, gamma=5.0 / 3.0, hlld_tol=1e-4,
                  domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0), device=0, steps_per_graph=0):
         L = load()
-        c = default_config()
-        c.nx, c.ny = nx, ny
-        c.x_min, c.x_max, c.y_min, c.y_max = domain
-        c.gamma, c.hlld_tol, c.cfl, c.alpha = gamma, hlld_tol, cfl, alpha
-        c.order = ORDER_MUSCL if order == "muscl" else ORDER_FIRST
-        c.solver = SOLVER_HLLD if solver == "hlld" else SOLVER_HLL
-        c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-        c.exact = int(bool(exact))
-        for k in range(4):
-            c.bc[k] = bc[k]
-        c.device = device
-        c.steps_per_graph = steps_per_graph
+        c = make_config(nx, ny, precision, exact, order, solver, cfl, alpha, gamma, hlld_tol, domain, bc,
+                        device, steps_per_graph)
         self.cfg = c
         self.dtype = np.float32 if c.precision == FP32 else np.float64
         h = ctypes.c_void_p()

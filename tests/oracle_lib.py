@@ -95,6 +95,13 @@ def lib():
             fn = getattr(_lib, "or_point_recon_" + name)
             fn.argtypes = [ptr] * 5
             fn.restype = None
+            ct = ctypes.c_double if name == "f64" else ctypes.c_float
+            fn = getattr(_lib, "or_point_minmod_" + name)
+            fn.argtypes = [ct, ct]
+            fn.restype = ct
+            fn = getattr(_lib, "or_point_positive_" + name)
+            fn.argtypes = [ptr, ctypes.c_double]
+            fn.restype = ctypes.c_int
     return _lib
 
 
