@@ -11,10 +11,11 @@
  * binary64 (suffix _f64) and binary32 (suffix _f32), plus a restatement of
  * this project's mixed-precision variant (suffix _mixed), which has no
  * counterpart in the reference:
- *   - state storage, primitive recovery from total energy, the flux
- *     divergence and the SSPRK2 accumulation in binary64;
- *   - reconstruction, the GLM+HLLD/HLL Riemann flux and the CFL signal speed
- *     in binary32.
+ *   - state storage, primitive recovery from total energy (one binary64
+ *     reciprocal of the density, then products), the SSPRK2 accumulation
+ *     and the flux divergence scaling in binary64;
+ *   - reconstruction, the GLM+HLLD/HLL Riemann flux, the difference of
+ *     neighbouring interface fluxes and the CFL signal speed in binary32.
  *
  * Pinning: the f64/f32 restatements are checked in tests/ against golden
  * vectors made by the reference's own headers and against output files of
@@ -76,14 +77,49 @@ static void or_mixed_face_states(const double* U, const float* P32, int c, int s
   or_prim9_to_state_f32(Pl1, UR, ph);
 }
 
+/* Binary64 primitive recovery of the mixed variant: density floor, one
+ * reciprocal of the density, velocities as products, pressure from total
+ * energy in the reference's association order. */
+static void or_mixed_prim9(const double* U, double* P, double gm1) {
+  double rho = or_max_f64(U[0], 1.0e-12);
+  double inv = 1.0 / rho;
+  double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
+  double bx = U[5], by = U[6], bz = U[7];
+  double v2 = vx * vx + vy * vy + vz * vz;
+  double b2 = bx * bx + by * by + bz * bz;
+  P[0] = rho; P[1] = vx; P[2] = vy; P[3] = vz;
+  P[4] = gm1 * (U[4] - 0.5 * rho * v2 - 0.5 * b2);
+  P[5] = bx; P[6] = by; P[7] = bz; P[8] = U[8];
+}
+
+/* stateIsUsable with the mixed recovery. */
+static int or_mixed_usable(const double* U, double gm1) {
+  double P[9];
+  if (U[0] <= 1.0e-12) return 0;
+  or_mixed_prim9(U, P, gm1);
+  return or_prim9_usable_f64(P);
+}
+
+static int or_mixed_all_usable(const double* U, int nx, int ny, int* bi, int* bj, double gm1) {
+  const int nxt = nx + 4;
+  int i, j;
+  for (j = 2; j < ny + 2; j++)
+    for (i = 2; i < nx + 2; i++)
+      if (!or_mixed_usable(&U[((size_t)j * nxt + i) * 9], gm1)) {
+        *bi = i - 2;
+        *bj = j - 2;
+        return 0;
+      }
+  return 1;
+}
+
 /* Binary64 recovery of every cell, rounded to binary32. */
-static void or_mixed_recover(const double* U, float* P32, size_t ncell,
-                             const or_phys_f64* ph64) {
+static void or_mixed_recover(const double* U, float* P32, size_t ncell, double gm1) {
   size_t c;
   int k;
   for (c = 0; c < ncell; c++) {
     double P[9];
-    or_state_to_prim9_f64(&U[c * 9], P, ph64);
+    or_mixed_prim9(&U[c * 9], P, gm1);
     for (k = 0; k < 9; k++) P32[c * 9 + k] = (float)P[k];
   }
 }
@@ -125,9 +161,9 @@ static void or_mixed_rhs(const double* Uc, const float* P32, double* rhs, float*
     for (i = G; i < nx + G; i++) {
       int id = j * nxt + i, im = id - 1, jm = id - nxt;
       for (k = 0; k < 9; k++) {
-        double dfx = (double)Fx[id * 9 + k] - (double)Fx[im * 9 + k];
-        double dgy = (double)Gy[id * 9 + k] - (double)Gy[jm * 9 + k];
-        rhs[id * 9 + k] = -dfx * inv_dx - dgy * inv_dy;
+        float dfx = Fx[id * 9 + k] - Fx[im * 9 + k];
+        float dgy = Gy[id * 9 + k] - Gy[jm * 9 + k];
+        rhs[id * 9 + k] = -(double)dfx * inv_dx - (double)dgy * inv_dy;
       }
       rhs[id * 9 + 8] -= damping * Uc[id * 9 + 8];
     }
@@ -145,10 +181,8 @@ static float or_mixed_max_speed(const float* P32, int nx, int ny, const or_phys_
 int or_run_mixed(const or_config* cfg, double* U, or_stats* st) {
   const int nx = cfg->nx, ny = cfg->ny, nxt = nx + 4;
   const size_t ncell = (size_t)nxt * (ny + 4), n = ncell * 9;
-  or_phys_f64 ph64;
   or_phys_f32 ph32;
-  ph64.gamma = cfg->gamma;
-  ph64.tol = cfg->hlld_tol;
+  const double gm1 = cfg->gamma - 1.0;
   ph32.gamma = (float)cfg->gamma;
   ph32.tol = (float)cfg->hlld_tol;
   const double dx = (cfg->x_max - cfg->x_min) / (double)nx;
@@ -165,14 +199,14 @@ int or_run_mixed(const or_config* cfg, double* U, or_stats* st) {
   memcpy(U1, U, n * sizeof(double));
   or_apply_bc_f64(U, nx, ny, cfg->bc);
   while (t < cfg->t_end && (cfg->max_steps < 0 || st->steps < cfg->max_steps)) {
-    or_mixed_recover(U, P32, ncell, &ph64);
+    or_mixed_recover(U, P32, ncell, gm1);
     float ch = or_max_f32(or_mixed_max_speed(P32, nx, ny, &ph32), 1.0e-12f);
     st->ch_last = (double)ch;
     double dt = cfg->cfl / ((double)ch / dx + (double)ch / dy);
     if (t + dt > cfg->t_end) dt = cfg->t_end - t;
     memcpy(Uc, U, n * sizeof(double));
     or_apply_bc_f64(Uc, nx, ny, cfg->bc);
-    or_mixed_recover(Uc, P32, ncell, &ph64);
+    or_mixed_recover(Uc, P32, ncell, gm1);
     or_mixed_rhs(Uc, P32, rhs, Fx, Gy, nx, ny, inv_dx, inv_dy, cfg->use_muscl,
                  cfg->use_hlld, ch, cfg->alpha, st, &ph32);
     for (j = 2; j < ny + 2; j++)
@@ -181,9 +215,9 @@ int or_run_mixed(const or_config* cfg, double* U, or_stats* st) {
         for (k = 0; k < 9; k++) U1[id + k] = U[id + k] + dt * rhs[id + k];
       }
     or_apply_bc_f64(U1, nx, ny, cfg->bc);
-    if (!or_all_usable_f64(U1, nx, ny, &st->bad_i, &st->bad_j, &ph64)) { rc = 3; break; }
+    if (!or_mixed_all_usable(U1, nx, ny, &st->bad_i, &st->bad_j, gm1)) { rc = 3; break; }
     memcpy(Uc, U1, n * sizeof(double));
-    or_mixed_recover(Uc, P32, ncell, &ph64);
+    or_mixed_recover(Uc, P32, ncell, gm1);
     or_mixed_rhs(Uc, P32, rhs, Fx, Gy, nx, ny, inv_dx, inv_dy, cfg->use_muscl,
                  cfg->use_hlld, ch, cfg->alpha, st, &ph32);
     for (j = 2; j < ny + 2; j++)
@@ -193,7 +227,7 @@ int or_run_mixed(const or_config* cfg, double* U, or_stats* st) {
           U[id + k] = 0.5 * U[id + k] + 0.5 * (U1[id + k] + dt * rhs[id + k]);
       }
     or_apply_bc_f64(U, nx, ny, cfg->bc);
-    if (!or_all_usable_f64(U, nx, ny, &st->bad_i, &st->bad_j, &ph64)) { rc = 4; break; }
+    if (!or_mixed_all_usable(U, nx, ny, &st->bad_i, &st->bad_j, gm1)) { rc = 4; break; }
     t += dt;
     st->steps++;
   }

@@ -20,6 +20,7 @@ enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
 
 // Arguments of one stage launch; the input planes come in as a TMA tensor map.
 struct StageArgs {
+  const void* u_in;   // stage input planes (U in stage 1, U1 in stage 2)
   void* u_out;        // stage output planes (U1 in stage 1, U in stage 2)
   const void* u_old;  // stage 2: U^n (the same buffer as u_out, read per cell)
   Ctrl* ctrl;

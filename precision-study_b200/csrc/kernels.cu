@@ -30,21 +30,37 @@ static cudaError_t init() {
   return init_pol<PolMixed>();
 }
 
+// Persistent grid: every SM holds as many stage CTAs as fit, capped by the
+// number of tiles.
+template <class Pol, int STAGE, bool HLLD>
+static int persistent_grid(int ntiles) {
+  static int per_sm = -1, sms = 0;
+  if (per_sm < 0) {
+    int dev = 0, nb = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage_kernel<Pol, STAGE, HLLD>, NT, Smem<Pol>::total);
+    per_sm = nb > 0 ? nb : 1;
+  }
+  const int g = sms * per_sm;
+  return g < ntiles ? g : ntiles;
+}
+
 template <class Pol>
 static cudaError_t launch_stage_pol(int hlld, int stage, const void* tmap_in, const StageArgs& a, cudaStream_t s) {
-  const dim3 grid((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
+  const int ntiles = ((a.nx + TX - 1) / TX) * ((a.ny + TY - 1) / TY);
   const size_t smem = Smem<Pol>::total;
   const CUtensorMap& tm = *static_cast<const CUtensorMap*>(tmap_in);
   if (hlld) {
     if (stage == 1)
-      stage_kernel<Pol, 1, true><<<grid, NT, smem, s>>>(tm, a);
+      stage_kernel<Pol, 1, true><<<persistent_grid<Pol, 1, true>(ntiles), NT, smem, s>>>(tm, a);
     else
-      stage_kernel<Pol, 2, true><<<grid, NT, smem, s>>>(tm, a);
+      stage_kernel<Pol, 2, true><<<persistent_grid<Pol, 2, true>(ntiles), NT, smem, s>>>(tm, a);
   } else {
     if (stage == 1)
-      stage_kernel<Pol, 1, false><<<grid, NT, smem, s>>>(tm, a);
+      stage_kernel<Pol, 1, false><<<persistent_grid<Pol, 1, false>(ntiles), NT, smem, s>>>(tm, a);
     else
-      stage_kernel<Pol, 2, false><<<grid, NT, smem, s>>>(tm, a);
+      stage_kernel<Pol, 2, false><<<persistent_grid<Pol, 2, false>(ntiles), NT, smem, s>>>(tm, a);
   }
   return cudaGetLastError();
 }

@@ -111,6 +111,7 @@ int make_tmap(pmhd_solver* s, void* base, CUtensorMap* tm) {
 
 StageArgs stage_args(const pmhd_solver* s, int stage, int parity) {
   StageArgs a;
+  a.u_in = stage == 1 ? s->dU : s->dU1;
   a.u_out = stage == 1 ? s->dU1 : s->dU;
   a.u_old = s->dU;
   a.ctrl = s->dCtrl;

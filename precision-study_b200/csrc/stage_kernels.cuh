@@ -7,7 +7,9 @@
 // for the next step's CFL reduction).  Per CTA and 32 x 8 output tile:
 //
 //   1. TMA loads the stage input tile with its 2-cell halo, all nine SoA
-//      planes, into shared memory (one 3-D box, no multicast).
+//      planes, into shared memory (one 3-D box, no multicast).  CTAs are
+//      persistent (SM count x resident CTAs) and load their next tile while
+//      they compute the current one.
 //   2. Every tile cell is recovered to primitives once (the reference
 //      recovers each cell up to 8 times, once per stencil use; the result of
 //      a recovery depends only on the cell, so this is bit-identical).
@@ -27,8 +29,9 @@
 // Precision policies:
 //   PolF64   storage, recovery, flux and update in binary64
 //   PolF32   storage, recovery, flux and update in binary32
-//   PolMixed storage, recovery, flux divergence and update in binary64;
-//            reconstruction, Riemann flux and CFL speed in binary32
+//   PolMixed storage, recovery (one reciprocal of the density), flux
+//            divergence scaling and update in binary64; reconstruction,
+//            Riemann flux, flux differences and CFL speed in binary32
 #ifndef PMHD_STAGE_KERNELS_CUH
 #define PMHD_STAGE_KERNELS_CUH
 
@@ -65,7 +68,10 @@ struct PolMixed {
   static constexpr bool kMixed = true;
 };
 
-constexpr int TX = 32, TY = 8;            // output tile
+#ifndef PMHD_TILE_Y
+#define PMHD_TILE_Y 8
+#endif
+constexpr int TX = 32, TY = PMHD_TILE_Y;  // output tile
 constexpr int HX = TX + 4, HY = TY + 4;   // tile with halo
 constexpr int TC = HX * HY;               // cells per loaded tile
 constexpr int NCELL = TX * TY;            // output cells per tile
@@ -79,16 +85,77 @@ static_assert(TX == 32, "one warp per tile row");
 
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 
+// Per-policy launch tuning, measured on B200 at Orszag-Tang 4096^2 (the
+// stage kernel is issue-bound, so these trade occupancy against registers
+// and shared memory):
+//   nbuf  input tile buffers: 1 = the next tile's TMA load reuses the buffer
+//         as soon as the current tile is recovered (the update then reads
+//         its own cell from global memory, an L2 hit); 2 = double buffering
+//         (the update reads shared memory);
+//   minb  resident CTAs per SM the register allocation is sized for.
+// fp64: 1 buffer, 2 CTAs (a small spill beats halving the resident warps);
+// fp32: 1 buffer, 3 CTAs; mixed: 2 buffers (its binary64 tile is large),
+// 2 CTAs.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64 override for tuning.
+template <class Pol>
+struct Tune {
+  static constexpr bool r64 = sizeof(typename Pol::R) == 8;
+#ifdef PMHD_NBUF
+  static constexpr int nbuf = PMHD_NBUF;
+#else
+  static constexpr int nbuf = Pol::kMixed ? 2 : 1;
+#endif
+#if defined(PMHD_MINB_R32) && defined(PMHD_MINB_R64)
+  static constexpr int minb = r64 ? PMHD_MINB_R64 : PMHD_MINB_R32;
+#elif defined(PMHD_MINB_R32)
+  static constexpr int minb = r64 ? 2 : PMHD_MINB_R32;
+#elif defined(PMHD_MINB_R64)
+  static constexpr int minb = r64 ? PMHD_MINB_R64 : (Pol::kMixed ? 2 : 3);
+#else
+  static constexpr int minb = r64 ? 2 : (Pol::kMixed ? 2 : 3);
+#endif
+};
+
 template <class Pol>
 struct Smem {
   using S = typename Pol::S;
   using R = typename Pol::R;
+  static constexpr int NBUF = Tune<Pol>::nbuf;
   static constexpr size_t u_bytes = sizeof(S) * NVAR * TC;  // TMA box size
-  static constexpr size_t p_off = align128(u_bytes);
+  static constexpr size_t u_stride = align128(u_bytes);      // per buffer
+  static constexpr size_t p_off = u_stride * NBUF;
   static constexpr size_t fx_off = p_off + align128(sizeof(R) * NVAR * TC);
   static constexpr size_t gy_off = fx_off + align128(sizeof(R) * NVAR * FXN);
   static constexpr size_t total = gy_off + align128(sizeof(R) * NVAR * GYN);
 };
+
+// Primitive recovery of one cell in the storage precision.  PolF64/PolF32
+// follow the reference (stateToPrimitiveDev, mhd2d_glm_gpu.cu:53-58: three
+// divisions by the density).  PolMixed is this project's variant: one
+// binary64 reciprocal of the density and three products, the pressure from
+// total energy in the reference's association order.
+template <class Pol>
+__device__ __forceinline__ void recover_cell(const typename Pol::S* U, typename Pol::S* P,
+                                             const Phys<typename Pol::S>& ph) {
+  if constexpr (Pol::kMixed) {
+    const double rho = fmax(U[RHO], 1.0e-12);
+    const double inv = 1.0 / rho;
+    const double vx = U[MX] * inv, vy = U[MY] * inv, vz = U[MZ] * inv;
+    const double bx = U[BX], by = U[BY], bz = U[BZ];
+    const double v2 = vx * vx + vy * vy + vz * vz;
+    const double b2 = bx * bx + by * by + bz * bz;
+    P[RHO] = rho;
+    P[MX] = vx;
+    P[MY] = vy;
+    P[MZ] = vz;
+    P[EN] = ph.gm1 * (U[EN] - 0.5 * rho * v2 - 0.5 * b2);
+    P[BX] = bx;
+    P[BY] = by;
+    P[BZ] = bz;
+    P[PSI] = U[PSI];
+  } else {
+    state_to_prim9<typename Pol::S>(U, P, ph);
+  }
+}
 
 // Ghost copies of interior index i (0 <= i < n) along one axis, in ghosted
 // coordinates, with whether the copy is a mirror image (reflecting wall).
@@ -144,19 +211,33 @@ __device__ __forceinline__ void store_cell(S* u, long long plane, int pitch, int
     }
 }
 
-// Face states and Riemann flux of one interface.  `base` is the tile index
-// of the cell two steps upwind of the interface; `stride` is 1 (x) or HX (y).
-template <class Pol, int AX, bool HLLD>
-__device__ __forceinline__ int face_flux(const typename Pol::S* sU, const typename Pol::R* sP, int base,
-                                         int stride, int muscl, typename Pol::R ch,
-                                         const Phys<typename Pol::R>& ph, typename Pol::R* F) {
+// Face states and Riemann flux of one interface, always computed in x-normal
+// slot order, from the tile's primitives in shared memory (MUSCL) or its
+// conserved states (first order).  A y-interface is solved exactly as the reference solves it:
+// the stencil is read with the x and y slots of velocity/momentum and field
+// swapped (mhdRotateYToX, mhd_common.hpp:381-391), the x-direction routine
+// runs, and the caller stores the flux back through the same swap
+// (mhdRotateFluxXToY, :395-405).  Reconstruction is per component and the
+// primitive->conserved sums are order-independent, so this equals the
+// reference bit for bit.  One copy of the flux code then serves both
+// directions, which keeps the kernel's hot loop inside the instruction cache.
+//   base   tile index of the cell two steps upwind of the interface
+//   stride 1 (x) or HX (y)
+//   o1/o2  plane offsets of the normal / first tangential velocity slot
+//   o5/o6  plane offsets of the normal / first tangential field slot
+template <class Pol, bool HLLD>
+__device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, int stride, int o1, int o2, int o5,
+                                         int o6, int muscl,
+                                         typename Pol::R ch, const Phys<typename Pol::R>& ph,
+                                         typename Pol::R* F) {
   using R = typename Pol::R;
+  const int off[NVAR] = {0, o1, o2, 3 * TC, 4 * TC, o5, o6, 7 * TC, 8 * TC};
   R UL[NVAR], UR[NVAR];
   if (muscl) {
     R Pm[NVAR], P0[NVAR], P1[NVAR], P2[NVAR], Pl[NVAR], Pr[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
-      const R* q = sP + k * TC + base;
+      const R* q = sP + off[k] + base;
       Pm[k] = q[0];
       P0[k] = q[stride];
       P1[k] = q[2 * stride];
@@ -166,42 +247,34 @@ __device__ __forceinline__ int face_flux(const typename Pol::S* sU, const typena
     prim9_to_state<R>(Pr, UL, ph);
     recon_cell<R>(P0, P1, P2, Pl, Pr);
     prim9_to_state<R>(Pl, UR, ph);
-  } else {
+  } else {  // first order: sP holds the conserved states
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
-      UL[k] = (R)sU[k * TC + base + stride];
-      UR[k] = (R)sU[k * TC + base + 2 * stride];
+      UL[k] = sP[off[k] + base + stride];
+      UR[k] = sP[off[k] + base + 2 * stride];
     }
   }
-  return glm_flux<R, AX>(UL, UR, ch, HLLD, F, ph);
+  return glm_flux<R, 0>(UL, UR, ch, HLLD, F, ph);
 }
 
-// Resident CTAs per SM the register allocation is sized for: two for the
-// binary32-flux policies; one for binary64, whose HLLD needs more registers
-// than two resident CTAs leave per thread (spilling costs more than the lost
-// occupancy).
-template <class Pol>
-struct StageMinBlocks {
-  static constexpr int value = sizeof(typename Pol::R) == 8 ? 1 : 2;
-};
-
 template <class Pol, int STAGE, bool HLLD>
-__global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
+__global__ void __launch_bounds__(NT, Tune<Pol>::minb)
     stage_kernel(const __grid_constant__ CUtensorMap tmap_in, const StageArgs a) {
   using S = typename Pol::S;
   using R = typename Pol::R;
   using TT = typename Pol::TT;
+  constexpr int NBUF = Tune<Pol>::nbuf;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  S* sU = reinterpret_cast<S*>(smem_raw);
   R* sP = reinterpret_cast<R*>(smem_raw + Smem<Pol>::p_off);
   R* sFx = reinterpret_cast<R*>(smem_raw + Smem<Pol>::fx_off);
   R* sGy = reinterpret_cast<R*>(smem_raw + Smem<Pol>::gy_off);
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[NBUF];
   __shared__ unsigned long long red_speed[NW];
   __shared__ unsigned red_deg[NW], red_np[NW];
+  auto ubuf = [&](int b) { return reinterpret_cast<S*>(smem_raw + (size_t)b * Smem<Pol>::u_stride); };
 
   const int tid = threadIdx.x;
-  const bool leader = (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0);
+  const bool leader = (blockIdx.x == 0 && tid == 0);
   Ctrl* c = a.ctrl;
   const int p = a.parity;
 
@@ -234,137 +307,173 @@ __global__ void __launch_bounds__(NT, StageMinBlocks<Pol>::value)
   const TT t_end = (TT)c->t_end;
   if (t + dt > t_end) dt = t_end - t;
 
-  // ---- 1. TMA tile load ---------------------------------------------------
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  // ---- persistent loop over tiles, next tile's TMA load in flight ---------
+  // The CTA owns tiles blockIdx.x, blockIdx.x + gridDim.x, ...  As soon as a
+  // tile's cells are recovered into sP, sU is free and the next tile's load
+  // is issued, so the load overlaps this tile's flux and update phases.
+  const int tiles_x = (a.nx + TX - 1) / TX;
+  const int ntiles = tiles_x * ((a.ny + TY - 1) / TY);
+  int tile = blockIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  unsigned n_deg = 0, n_np = 0;
+  unsigned long long sp_bits = 0;
+  const S* u_in = static_cast<const S*>(a.u_in);
   if (tid == 0) {
-    mbar_init(&bar, 1);
+    for (int b = 0; b < NBUF; b++) mbar_init(&bar[b], 1);
     fence_barrier_init();
   }
   __syncthreads();
-  if (tid == 0) {
-    mbar_arrive_expect_tx(&bar, (uint32_t)Smem<Pol>::u_bytes);
-    tma_load_3d(sU, &tmap_in, &bar, i0, j0, 0);
+  if (tid == 0 && tile < ntiles) {
+    mbar_arrive_expect_tx(&bar[0], (uint32_t)Smem<Pol>::u_bytes);
+    tma_load_3d(ubuf(0), &tmap_in, &bar[0], (tile % tiles_x) * TX, (tile / tiles_x) * TY, 0);
   }
-  const bool got = __syncthreads_and(mbar_wait_bounded(&bar, 0, kWaitIters));
-  if (!got) {
-    if (tid == 0) atomicExch(&c->err, (int)DERR_TMA_TIMEOUT);
-    mbar_wait_bounded(&bar, 0, kWaitIters);  // let the copy land before leaving
-    return;
-  }
+  for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {
+    const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
+    const int cb = it % NBUF;                        // buffer of this tile
+    const uint32_t par = (uint32_t)(it / NBUF) & 1;  // its mbarrier phase
+    S* sU = ubuf(cb);
+    const bool got = __syncthreads_and(mbar_wait_bounded(&bar[cb], par, kWaitIters));
+    if (!got) {
+      if (tid == 0) atomicExch(&c->err, (int)DERR_TMA_TIMEOUT);
+      mbar_wait_bounded(&bar[cb], par, kWaitIters);  // let the copy land before leaving
+      return;
+    }
 
-  // ---- 2. recovery, once per tile cell (halo corners are never used) -------
-  if (a.muscl) {
+    // ---- recovery, once per tile cell (halo corners are never used) -------
+    // First order needs no primitives: the conserved states are staged.
     for (int q = tid; q < TC; q += NT) {
       const int cx = q % HX, cy = q / HX;
       if ((cx < 2 || cx >= TX + 2) && (cy < 2 || cy >= TY + 2)) continue;
       S U9[NVAR], P9[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) U9[k] = sU[k * TC + q];
-      state_to_prim9<S>(U9, P9, phS);
+      if (a.muscl) {
+        recover_cell<Pol>(U9, P9, phS);
+      } else {
+#pragma unroll
+        for (int k = 0; k < NVAR; k++) P9[k] = U9[k];
+      }
 #pragma unroll
       for (int k = 0; k < NVAR; k++) sP[k * TC + q] = (R)P9[k];
     }
     __syncthreads();
-  }
-
-  // ---- 3. interface fluxes --------------------------------------------------
-  // Warps 0..TY-1 own one tile row each: lane tx computes the x-interface to
-  // the right of cell (tx, ty), then the y-interface above it.  The last warp
-  // computes the tile's bottom row of y-interfaces, then its left column of
-  // x-interfaces.  Every warp runs two rounds of one direction each, so no
-  // warp lags at the barrier and no warp mixes the two code paths.
-  const int warp = tid >> 5, lane = tid & 31;
-  unsigned n_deg = 0, n_np = 0;
-  auto x_face = [&](int fx, int fy) {
-    const int gi = i0 + fx;  // interface between cells gi-1 and gi
-    if (gi > a.nx || j0 + fy >= a.ny) return;
-    R F[NVAR];
-    const int st = face_flux<Pol, 0, HLLD>(sU, sP, (fy + 2) * HX + fx, 1, a.muscl, ch, phR, F);
-#pragma unroll
-    for (int k = 0; k < NVAR; k++) sFx[k * FXN + fy * (TX + 1) + fx] = F[k];
-    if (HLLD && (fx >= 1 || i0 == 0)) {
-      n_deg += (st == HLLD_FALLBACK_DEGENERATE);
-      n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
+    // The next tile goes into the buffer no thread reads any more: this
+    // one (just recovered) or, double-buffered, the previous tile's.
+    if (tid == 0 && tile + (int)gridDim.x < ntiles) {
+      const int nt = tile + gridDim.x, nb = (it + 1) % NBUF;
+      fence_proxy_async_smem();  // order earlier reads of that buffer before the async overwrite
+      mbar_arrive_expect_tx(&bar[nb], (uint32_t)Smem<Pol>::u_bytes);
+      tma_load_3d(ubuf(nb), &tmap_in, &bar[nb], (nt % tiles_x) * TX, (nt / tiles_x) * TY, 0);
     }
-  };
-  auto y_face = [&](int fx, int fy) {
-    const int gj = j0 + fy;  // interface between rows gj-1 and gj
-    if (gj > a.ny || i0 + fx >= a.nx) return;
-    R F[NVAR];
-    const int st = face_flux<Pol, 1, HLLD>(sU, sP, fy * HX + fx + 2, HX, a.muscl, ch, phR, F);
-#pragma unroll
-    for (int k = 0; k < NVAR; k++) sGy[k * GYN + fy * TX + fx] = F[k];
-    if (HLLD && (fy >= 1 || j0 == 0)) {
-      n_deg += (st == HLLD_FALLBACK_DEGENERATE);
-      n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
-    }
-  };
-  if (warp < TY) {
-    x_face(lane + 1, warp);
-    y_face(lane, warp + 1);
-  } else {
-    y_face(lane, 0);
-    if (lane < TY) x_face(0, lane);
-  }
-  __syncthreads();
 
-  // ---- 4. divergence, update, checks, store, next-step speed ---------------
-  const int tx = lane, ty = warp;
-  const int gi = i0 + tx, gj = j0 + ty;
-  unsigned long long sp_bits = 0;
-  if (warp < TY && gi < a.nx && gj < a.ny) {
-    const int lc = (ty + 2) * HX + (tx + 2);
-    const size_t gidx = (size_t)(gj + GHOST) * a.pitch + (gi + GHOST);
-    S Un[NVAR];
-    if constexpr (!Pol::kMixed) {
-      // Reference order (mhd2d_glm_gpu.cu:282-285, :299, :316-317).
-      const R damping = ch / vmax((R)a.alpha, (R)1.0e-12);
-#pragma unroll
-      for (int k = 0; k < NVAR; k++) {
-        const R uin = sU[k * TC + lc];
-        R rhs = -(sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx]) / (R)dxT -
-                (sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx]) / (R)dyT;
-        if (k == PSI) rhs -= damping * uin;
-        if (STAGE == 1) {
-          Un[k] = uin + (R)dt * rhs;
-        } else {
-          const S uold = static_cast<const S*>(a.u_old)[(size_t)k * a.plane + gidx];
-          Un[k] = (R)0.5 * uold + (R)0.5 * (uin + (R)dt * rhs);
-        }
+    // ---- interface fluxes --------------------------------------------------
+    // Warps 0..TY-1 own one tile row each: lane tx computes the x-interface
+    // to the right of cell (tx, ty), then the y-interface above it.  The last
+    // warp computes the tile's bottom row of y-interfaces, then its left
+    // column of x-interfaces.  Every warp runs two rounds, each round one
+    // direction for the whole warp, through one (not unrolled) copy of the
+    // flux code.
+#pragma unroll 1
+    for (int r = 0; r < 2; r++) {
+      int axis, fx, fy;
+      if (warp < TY) {
+        axis = r;
+        fx = r ? lane : lane + 1;
+        fy = r ? warp + 1 : warp;
+      } else {
+        axis = 1 - r;
+        fx = r ? 0 : lane;
+        fy = r ? lane : 0;
+        if (r == 1 && lane >= TY) continue;
       }
-    } else {
-      // Binary32 fluxes, binary64 divergence and accumulation.
-      const double damping = (double)ch / fmax(a.alpha, 1.0e-12);
-      const double inv_dx = 1.0 / a.dx, inv_dy = 1.0 / a.dy;
-#pragma unroll
-      for (int k = 0; k < NVAR; k++) {
-        const double uin = sU[k * TC + lc];
-        const double dfx = (double)sFx[k * FXN + ty * (TX + 1) + tx + 1] - (double)sFx[k * FXN + ty * (TX + 1) + tx];
-        const double dgy = (double)sGy[k * GYN + (ty + 1) * TX + tx] - (double)sGy[k * GYN + ty * TX + tx];
-        double rhs = -dfx * inv_dx - dgy * inv_dy;
-        if (k == PSI) rhs -= damping * uin;
-        if (STAGE == 1) {
-          Un[k] = uin + (double)dt * rhs;
-        } else {
-          const double uold = static_cast<const double*>(a.u_old)[(size_t)k * a.plane + gidx];
-          Un[k] = 0.5 * uold + 0.5 * (uin + (double)dt * rhs);
-        }
+      // x: interface between cells (i0+fx-1, j0+fy) and (i0+fx, j0+fy)
+      // y: interface between cells (i0+fx, j0+fy-1) and (i0+fx, j0+fy)
+      const bool valid = axis ? (j0 + fy <= a.ny && i0 + fx < a.nx) : (i0 + fx <= a.nx && j0 + fy < a.ny);
+      if (!valid) continue;
+      const int base = axis ? fy * HX + fx + 2 : (fy + 2) * HX + fx;
+      const int stride = axis ? HX : 1;
+      const int o1 = (axis ? 2 : 1) * TC, o2 = (axis ? 1 : 2) * TC;
+      const int o5 = (axis ? 6 : 5) * TC, o6 = (axis ? 5 : 6) * TC;
+      R F[NVAR];
+      const int st = face_flux<Pol, HLLD>(sP, base, stride, o1, o2, o5, o6, a.muscl, ch, phR, F);
+      R* out = axis ? sGy : sFx;
+      const int n_out = axis ? GYN : FXN;
+      const int item = axis ? fy * TX + fx : fy * (TX + 1) + fx;
+      const int p1 = axis ? 2 : 1, p2 = axis ? 1 : 2, p5 = axis ? 6 : 5, p6 = axis ? 5 : 6;
+      out[0 * n_out + item] = F[0];
+      out[p1 * n_out + item] = F[1];
+      out[p2 * n_out + item] = F[2];
+      out[3 * n_out + item] = F[3];
+      out[4 * n_out + item] = F[4];
+      out[p5 * n_out + item] = F[5];
+      out[p6 * n_out + item] = F[6];
+      out[7 * n_out + item] = F[7];
+      out[8 * n_out + item] = F[8];
+      if (HLLD && ((axis ? fy : fx) >= 1 || (axis ? j0 : i0) == 0)) {
+        n_deg += (st == HLLD_FALLBACK_DEGENERATE);
+        n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
       }
     }
-    // stateIsUsable (mhd2d_glm_gpu.cu:74-79); its recovery doubles as the
-    // recovery of the next step's CFL speed (speedKernel, :171-195).
-    S P9[NVAR];
-    state_to_prim9<S>(Un, P9, phS);
-    if (!(Un[RHO] > rho_floor<S>()) || !prim9_usable<S>(P9)) {
-      atomicMin(STAGE == 1 ? &c->bad1 : &c->bad2, gj * a.nx + gi);
-      c->bad_step = step;
-    }
-    store_cell<S>(static_cast<S*>(a.u_out), a.plane, a.pitch, gi, gj, a.nx, a.ny, a.bc, Un);
-    if (STAGE == 2) {
-      R Pr[NVAR];
+    __syncthreads();
+
+    // ---- divergence, update, checks, store, next-step speed ---------------
+    const int tx = lane, ty = warp;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (warp < TY && gi < a.nx && gj < a.ny) {
+      const size_t gidx = (size_t)(gj + GHOST) * a.pitch + (gi + GHOST);
+      S Un[NVAR];
+      if constexpr (!Pol::kMixed) {
+        // Reference order (mhd2d_glm_gpu.cu:282-285, :299, :316-317).
+        const R damping = ch / vmax((R)a.alpha, (R)1.0e-12);
 #pragma unroll
-      for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
-      sp_bits = speed_bits((double)cell_speed<R>(Pr, phR));
+        for (int k = 0; k < NVAR; k++) {
+          const R uin = NBUF == 2 ? sU[k * TC + (ty + 2) * HX + tx + 2] : u_in[(size_t)k * a.plane + gidx];
+          R rhs = -(sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx]) / (R)dxT -
+                  (sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx]) / (R)dyT;
+          if (k == PSI) rhs -= damping * uin;
+          if (STAGE == 1) {
+            Un[k] = uin + (R)dt * rhs;
+          } else {
+            const S uold = static_cast<const S*>(a.u_old)[(size_t)k * a.plane + gidx];
+            Un[k] = (R)0.5 * uold + (R)0.5 * (uin + (R)dt * rhs);
+          }
+        }
+      } else {
+        // Binary32 fluxes and their differences, binary64 scaling and
+        // accumulation.
+        const double damping = (double)ch / fmax(a.alpha, 1.0e-12);
+        const double inv_dx = 1.0 / a.dx, inv_dy = 1.0 / a.dy;
+#pragma unroll
+        for (int k = 0; k < NVAR; k++) {
+          const double uin = NBUF == 2 ? sU[k * TC + (ty + 2) * HX + tx + 2] : u_in[(size_t)k * a.plane + gidx];
+          const float dfx = sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx];
+          const float dgy = sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx];
+          double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
+          if (k == PSI) rhs -= damping * uin;
+          if (STAGE == 1) {
+            Un[k] = uin + (double)dt * rhs;
+          } else {
+            const double uold = static_cast<const double*>(a.u_old)[(size_t)k * a.plane + gidx];
+            Un[k] = 0.5 * uold + 0.5 * (uin + (double)dt * rhs);
+          }
+        }
+      }
+      // stateIsUsable (mhd2d_glm_gpu.cu:74-79); its recovery doubles as the
+      // recovery of the next step's CFL speed (speedKernel, :171-195).
+      S P9[NVAR];
+      recover_cell<Pol>(Un, P9, phS);
+      if (!(Un[RHO] > rho_floor<S>()) || !prim9_usable<S>(P9)) {
+        atomicMin(STAGE == 1 ? &c->bad1 : &c->bad2, gj * a.nx + gi);
+        c->bad_step = step;
+      }
+      store_cell<S>(static_cast<S*>(a.u_out), a.plane, a.pitch, gi, gj, a.nx, a.ny, a.bc, Un);
+      if (STAGE == 2) {
+        R Pr[NVAR];
+#pragma unroll
+        for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
+        const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, phR));
+        sp_bits = b > sp_bits ? b : sp_bits;
+      }
     }
   }
 
@@ -429,7 +538,7 @@ __global__ void __launch_bounds__(NTA) speed_kernel(const typename Pol::S* __res
     R Pr[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) U9[k] = u[(size_t)k * plane + g];
-    state_to_prim9<S>(U9, P9, phS);
+    recover_cell<Pol>(U9, P9, phS);
 #pragma unroll
     for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
     const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, phR));
