@@ -168,6 +168,30 @@ const char* pmhd_strerror(int status);
 /* Copies the configuration a handle was created with. */
 int pmhd_get_config(const pmhd_solver* s, pmhd_config* cfg);
 
+/* ---- Allocation-free time loop ----------------------------------------------
+ * No counterpart in the reference: its program always cudaMallocs five state
+ * arrays.  For callers that must not allocate device memory while they run
+ * (a process that pre-carves all GPU memory into its own pool, an allocator
+ * hook that forbids cudaMalloc after start-up, a fixed memory plan that must
+ * not fail mid-run).  Advances the caller's state like pmhd_advance, but with
+ * no handle and no allocation: d_in and d_out are the caller's DEVICE buffers
+ * of ny*nx*9 elements in the PMHD_LAYOUT_INTERIOR order (double for fp64 and
+ * mixed, float for fp32; they may be the same buffer); t0 and step0 are the
+ * time and step count d_in is at; stream is a cudaStream_t (NULL = the
+ * default stream).  The working state lives in one array compiled into the
+ * library, PMHD_NOALLOC_SCRATCH_BYTES long, that every GPU loading the
+ * library keeps until exit.  Grids whose working state does not fit --
+ * 256 + 2 * round_up_256(9 * (ny+4) * round_up(nx+4, 16) * element size)
+ * bytes, up to 586^2 cells in fp64/mixed and 828^2 in fp32 -- are rejected
+ * with PMHD_ERR_UNSUPPORTED.  All calls share that array: calls that overlap
+ * on the GPU race; serialise them.  The first call on a device sets it up
+ * (looks up the array's address with that device current); make it before
+ * any stream capture.  stats: as pmhd_advance (steps/t are totals including
+ * step0/t0; device_ms is not measured, 0). */
+#define PMHD_NOALLOC_SCRATCH_BYTES (48u << 20)
+int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, void* d_out, double t0, long long step0,
+                         double t_end, long long max_steps, void* stream, pmhd_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

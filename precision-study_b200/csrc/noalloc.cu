@@ -1,0 +1,281 @@
+// noalloc.cu -- pmhd_advance_noalloc: the time loop without any device
+// allocation.
+//
+// Who needs it: code that must not allocate GPU memory while it runs --
+// for example a caller that has carved all device memory into its own pool
+// up front (a serving process or a coupled multiphysics code with a fixed
+// memory plan), a caller running under an allocator hook that forbids
+// cudaMalloc after start-up, or code that must not risk an allocation
+// failure half way through a run.  The regular path (pmhd_create) allocates
+// two state buffers and a control block per handle; this entry point
+// instead works on the caller's own device buffers and keeps its working
+// state -- the stage-1 state, the step state in the solver's padded planar
+// layout and the control block -- in one fixed array compiled into the
+// library (`g_noalloc_scratch`, 48 MiB, see PMHD_NOALLOC_SCRATCH_BYTES).
+//
+// Properties (also stated in include/pmhd.h):
+//   * The array is a static __device__ object: every GPU that loads this
+//     library holds it until the process exits.
+//   * Grids are limited to what fits in it: 256 bytes of control block plus
+//     two states of 9 x (ny + 4) x round_up(nx + 4, 16) elements (8 bytes in
+//     fp64 / mixed, 4 in fp32), each rounded up to 256 bytes.  Up to 586^2
+//     cells in fp64 / mixed and 828^2 in fp32.  Larger grids are rejected
+//     with PMHD_ERR_UNSUPPORTED before anything is launched.
+//   * Every call shares the array and it keeps the last call's contents;
+//     each call rewrites the control block and the whole state before using
+//     them.  Calls that overlap on the GPU (from several host threads or
+//     streams at once) race on the array and give wrong results: serialise
+//     them.
+//   * The first call on a device looks up the array's device address
+//     (cudaGetSymbolAddress) and sets the kernels' shared-memory limits,
+//     with that device current; make that first call before any stream
+//     capture.
+//   * It calls no cudaMalloc / cudaFree / graph instantiation and no library
+//     routine that allocates: kernels are launched directly on the caller's
+//     stream and the control block is read back into a host stack variable.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+#include "kernel_api.h"
+#include "pmhd.h"
+
+using namespace pmhd;
+
+namespace {
+
+constexpr size_t kScratchBytes = (size_t)PMHD_NOALLOC_SCRATCH_BYTES;
+constexpr size_t kCtrlBytes = 256;
+static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block must fit its slot");
+
+// The fixed working memory of pmhd_advance_noalloc (see the file comment).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+struct DeviceSetup {
+  bool done = false;
+  unsigned char* base = nullptr;  // device address of g_noalloc_scratch
+};
+std::mutex g_mu;
+DeviceSetup g_setup[64];
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Same validation as pmhd_create.
+bool config_ok(const pmhd_config* c) {
+  if (!c || c->nx < 4 || c->ny < 4 || (long long)c->nx * c->ny > (long long)INT_MAX) return false;
+  if (!(c->x_max > c->x_min) || !(c->y_max > c->y_min)) return false;
+  if (!(c->cfl > 0.0) || !(c->cfl < 1.0) || !(c->alpha > 0.0) || !(c->gamma > 1.0)) return false;
+  if (!(c->hlld_tol >= 0.0)) return false;
+  if (c->order != PMHD_ORDER_FIRST && c->order != PMHD_ORDER_MUSCL) return false;
+  if (c->solver != PMHD_SOLVER_HLL && c->solver != PMHD_SOLVER_HLLD) return false;
+  if (c->precision < PMHD_FP64 || c->precision > PMHD_MIXED) return false;
+  for (int k = 0; k < 4; k++)
+    if (c->bc[k] < PMHD_BC_PERIODIC || c->bc[k] > PMHD_BC_TRANSMISSIVE) return false;
+  if ((c->bc[0] == PMHD_BC_PERIODIC) != (c->bc[1] == PMHD_BC_PERIODIC)) return false;
+  if ((c->bc[2] == PMHD_BC_PERIODIC) != (c->bc[3] == PMHD_BC_PERIODIC)) return false;
+  return true;
+}
+
+// Once per device, with that device current: the array's device address
+// and the kernels' shared-memory attributes.
+int setup_device(int dev, unsigned char** base) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceSetup& d = g_setup[dev & 63];
+  if (!d.done) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return PMHD_ERR_CUDA;
+    if (kernel_table_exact().init() != cudaSuccess || kernel_table_fast().init() != cudaSuccess)
+      return PMHD_ERR_CUDA;
+    d.base = static_cast<unsigned char*>(p);
+    d.done = true;
+  }
+  *base = d.base;
+  return PMHD_OK;
+}
+
+int make_tmap(const KernelTable& kt, int precision, int nx, int ny, int pitch, long long plane, size_t elem,
+              void* base, CUtensorMap* tm) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return PMHD_ERR_CUDA;
+  int tx, ty;
+  size_t smem;
+  kt.tile(precision, &tx, &ty, &smem);
+  const cuuint64_t dims[3] = {(cuuint64_t)nx + 4, (cuuint64_t)ny + 4, 9};
+  const cuuint64_t strides[2] = {(cuuint64_t)pitch * elem, (cuuint64_t)plane * elem};
+  const cuuint32_t box[3] = {(cuuint32_t)tx + 4, (cuuint32_t)ty + 4, 9};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(tm, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? PMHD_OK : PMHD_ERR_CUDA;
+}
+
+}  // namespace
+
+namespace {
+size_t scratch_needed(const pmhd_config* cfg) {
+  const size_t elem = cfg->precision == PMHD_FP32 ? 4 : 8;
+  const size_t pitch = ((size_t)(cfg->nx + 4) + 15) / 16 * 16;
+  const size_t plane = pitch * (size_t)(cfg->ny + 4);
+  return kCtrlBytes + 2 * round256(9 * plane * elem);
+}
+}  // namespace
+
+extern "C" int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, void* d_out, double t0,
+                                    long long step0, double t_end, long long max_steps, void* stream,
+                                    pmhd_stats* stats) {
+  if (!config_ok(cfg) || !d_in || !d_out || std::isnan(t_end) || !std::isfinite(t0) || step0 < 0)
+    return PMHD_ERR_ARG;
+  if (scratch_needed(cfg) > kScratchBytes) return PMHD_ERR_UNSUPPORTED;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return PMHD_ERR_NODEVICE;
+  if (prop.major != 10 || prop.minor != 0) return PMHD_ERR_NODEVICE;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return PMHD_ERR_CUDA;
+  unsigned char* base = nullptr;
+  int rc = setup_device(cfg->device, &base);
+  if (rc != PMHD_OK) return rc;
+
+  const bool f32 = cfg->precision == PMHD_FP32;
+  const size_t elem = f32 ? 4 : 8;
+  const int nx = cfg->nx, ny = cfg->ny;
+  const int pitch = ((nx + 4) + 15) / 16 * 16;
+  const long long plane = (long long)pitch * (ny + 4);
+  Ctrl* dctrl = reinterpret_cast<Ctrl*>(base);
+  void* dU = base + kCtrlBytes;
+  void* dU1 = base + kCtrlBytes + round256(9 * (size_t)plane * elem);
+  const KernelTable& kt = cfg->exact ? kernel_table_exact() : kernel_table_fast();
+  CUtensorMap tmU, tmU1;
+  if ((rc = make_tmap(kt, cfg->precision, nx, ny, pitch, plane, elem, dU, &tmU)) != PMHD_OK) return rc;
+  if ((rc = make_tmap(kt, cfg->precision, nx, ny, pitch, plane, elem, dU1, &tmU1)) != PMHD_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  // Values the reference holds in its Real type.
+  auto tt = [&](double v) { return f32 ? (double)(float)v : v; };
+  double dx, dy;
+  if (f32) {
+    dx = (double)(((float)cfg->x_max - (float)cfg->x_min) / (float)nx);
+    dy = (double)(((float)cfg->y_max - (float)cfg->y_min) / (float)ny);
+  } else {
+    dx = (cfg->x_max - cfg->x_min) / (double)nx;
+    dy = (cfg->y_max - cfg->y_min) / (double)ny;
+  }
+
+  // Control block: everything that must start at zero is rewritten here.
+  Ctrl h;
+  std::memset(&h, 0, sizeof(h));
+  h.t[0] = h.t[1] = tt(t0);
+  h.step[0] = h.step[1] = step0;
+  h.t_end = tt(t_end);
+  h.step_limit = max_steps < 0 ? LLONG_MAX : step0 + max_steps;
+  h.bad1 = h.bad2 = BAD_NONE;
+#define PMHD_NA(call)                               \
+  do {                                              \
+    if ((call) != cudaSuccess) return PMHD_ERR_CUDA; \
+  } while (0)
+  PMHD_NA(cudaMemcpyAsync(dctrl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  PMHD_NA(kt.aos_to_soa(cfg->precision, d_in, PMHD_LAYOUT_INTERIOR, dU, plane, nx, ny, pitch, cfg->bc, s));
+  PMHD_NA(kt.speed(cfg->precision, dU, plane, nx, ny, pitch, cfg->gamma, dctrl, 0, s));
+
+  StageArgs a[2];
+  for (int st = 0; st < 2; st++) {
+    StageArgs& x = a[st];
+    x.u_in = st == 0 ? dU : dU1;
+    x.u_out = st == 0 ? dU1 : dU;
+    x.u_old = dU;
+    x.ctrl = dctrl;
+    x.plane = plane;
+    x.nx = nx;
+    x.ny = ny;
+    x.pitch = pitch;
+    x.muscl = cfg->order == PMHD_ORDER_MUSCL ? 1 : 0;
+    for (int k = 0; k < 4; k++) x.bc[k] = cfg->bc[k];
+    x.gamma = cfg->gamma;
+    x.tol = cfg->hlld_tol;
+    x.cfl = tt(cfg->cfl);
+    x.alpha = tt(cfg->alpha);
+    x.dx = dx;
+    x.dy = dy;
+  }
+  const int hlld = cfg->solver == PMHD_SOLVER_HLLD ? 1 : 0;
+  // Steps are launched in pairs (parity 0 then 1) so the final values land
+  // in control slot 0; a step past the stop condition is a no-op.
+  auto launch_pairs = [&](long long pairs) -> int {
+    for (long long q = 0; q < pairs; q++)
+      for (int par = 0; par < 2; par++) {
+        a[0].parity = a[1].parity = par;
+        if (kt.stage(cfg->precision, hlld, 1, &tmU, a[0], s) != cudaSuccess) return PMHD_ERR_CUDA;
+        if (kt.stage(cfg->precision, hlld, 2, &tmU1, a[1], s) != cudaSuccess) return PMHD_ERR_CUDA;
+      }
+    return PMHD_OK;
+  };
+  Ctrl r;
+  if (max_steps >= 0) {
+    if ((rc = launch_pairs((max_steps + 1) / 2)) != PMHD_OK) return rc;
+    PMHD_NA(cudaMemcpyAsync(&r, dctrl, sizeof(r), cudaMemcpyDeviceToHost, s));
+    PMHD_NA(cudaStreamSynchronize(s));
+  } else {
+    for (;;) {
+      if ((rc = launch_pairs(16)) != PMHD_OK) return rc;
+      PMHD_NA(cudaMemcpyAsync(&r, dctrl, sizeof(r), cudaMemcpyDeviceToHost, s));
+      PMHD_NA(cudaStreamSynchronize(s));
+      if (r.halted || r.err || r.bad1 != BAD_NONE || r.bad2 != BAD_NONE || !(r.t[0] < r.t_end)) break;
+    }
+  }
+  PMHD_NA(kt.soa_to_aos(cfg->precision, dU, plane, nx, ny, pitch, PMHD_LAYOUT_INTERIOR, d_out, s));
+  PMHD_NA(cudaStreamSynchronize(s));
+#undef PMHD_NA
+
+  int status = PMHD_OK;
+  long long stages = 2 * (r.step[0] - step0);
+  pmhd_stats out;
+  std::memset(&out, 0, sizeof(out));
+  out.bad_i = out.bad_j = -1;
+  out.bad_step = -1;
+  if (r.err) {
+    status = PMHD_ERR_TIMEOUT;
+  } else if (r.bad1 != BAD_NONE || r.bad2 != BAD_NONE) {
+    const int bad = r.bad1 != BAD_NONE ? r.bad1 : r.bad2;
+    status = r.bad1 != BAD_NONE ? PMHD_ERR_STAGE1 : PMHD_ERR_STAGE2;
+    stages += r.bad1 != BAD_NONE ? 1 : 2;
+    out.bad_i = bad % nx;
+    out.bad_j = bad / nx;
+    out.bad_step = r.bad_step;
+  }
+  out.steps = r.step[0];
+  out.t = r.t[0];
+  out.ch_last = r.last_ch;
+  out.dt_last = r.last_dt;
+  if (hlld) {
+    out.x_evals = (unsigned long long)stages * (unsigned long long)(nx + 1) * ny;
+    out.y_evals = (unsigned long long)stages * (unsigned long long)nx * (ny + 1);
+    out.degenerate = r.degenerate;
+    out.nonphysical = r.nonphysical;
+  }
+  out.kernel_launches = r.active_stage_launches + 1;
+  out.status = status;
+  if (stats) *stats = out;
+  return status;
+}

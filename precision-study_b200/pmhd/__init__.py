@@ -37,7 +37,7 @@ EXPORTS = (
     "pmhd_config_default", "pmhd_create", "pmhd_destroy", "pmhd_init_problem",
     "pmhd_set_state", "pmhd_get_state", "pmhd_set_time", "pmhd_advance",
     "pmhd_get_stats", "pmhd_diagnostics", "pmhd_write_dat", "pmhd_dat_filename",
-    "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state",
+    "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state", "pmhd_advance_noalloc",
 )
 
 
@@ -104,6 +104,7 @@ def load():
         "pmhd_strerror": ([i], ctypes.c_char_p),
         "pmhd_get_config": ([vp, P(Config)], i),
         "pmhd_problem_state": ([P(Config), i, P(d), i, vp], i),
+        "pmhd_advance_noalloc": ([P(Config), vp, vp, d, ctypes.c_longlong, d, ctypes.c_longlong, vp, P(Stats)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
