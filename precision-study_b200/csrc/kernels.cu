@@ -1,26 +1,42 @@
 // kernels.cu -- instantiates the pmhd kernels for every precision policy and
-// exposes them through a KernelTable.  Built twice by the Makefile:
+// tile height and exposes them through a KernelTable.  Built twice by the
+// Makefile:
 //   -DPMHD_KNS=exact -fmad=false                  -> kernel_table_exact()
 //   -DPMHD_KNS=fast  -fmad=true -prec-div=false -prec-sqrt=false
 //                                                 -> kernel_table_fast()
+#include <mutex>
+
 #include "stage_kernels.cuh"
 
 namespace pmhd {
 namespace PMHD_KNS {
 
-template <class Pol, int STAGE, bool HLLD>
+template <class Pol, int STAGE, bool HLLD, int TY, bool BATCHED>
 static cudaError_t set_smem_attr() {
-  return cudaFuncSetAttribute(stage_kernel<Pol, STAGE, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)Smem<Pol>::total);
+  return cudaFuncSetAttribute(stage_kernel<Pol, STAGE, HLLD, TY, BATCHED>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem<Pol, TY>::total);
+}
+
+template <class Pol, int TY, bool BATCHED>
+static cudaError_t init_pol_ty_b() {
+  cudaError_t e;
+  if ((e = set_smem_attr<Pol, 1, true, TY, BATCHED>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<Pol, 2, true, TY, BATCHED>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<Pol, 1, false, TY, BATCHED>()) != cudaSuccess) return e;
+  return set_smem_attr<Pol, 2, false, TY, BATCHED>();
+}
+
+template <class Pol, int TY>
+static cudaError_t init_pol_ty() {
+  cudaError_t e = init_pol_ty_b<Pol, TY, false>();
+  return e != cudaSuccess ? e : init_pol_ty_b<Pol, TY, true>();
 }
 
 template <class Pol>
 static cudaError_t init_pol() {
   cudaError_t e;
-  if ((e = set_smem_attr<Pol, 1, true>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<Pol, 2, true>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<Pol, 1, false>()) != cudaSuccess) return e;
-  return set_smem_attr<Pol, 2, false>();
+  if ((e = init_pol_ty<Pol, kTileHeights[0]>()) != cudaSuccess) return e;
+  return init_pol_ty<Pol, kTileHeights[1]>();
 }
 
 static cudaError_t init() {
@@ -30,48 +46,103 @@ static cudaError_t init() {
   return init_pol<PolMixed>();
 }
 
-// Persistent grid: every SM holds as many stage CTAs as fit, capped by the
-// number of tiles.
-template <class Pol, int STAGE, bool HLLD>
-static int persistent_grid(int ntiles) {
-  static int per_sm = -1, sms = 0;
-  if (per_sm < 0) {
-    int dev = 0, nb = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage_kernel<Pol, STAGE, HLLD>, NT, Smem<Pol>::total);
-    per_sm = nb > 0 ? nb : 1;
-  }
-  const int g = sms * per_sm;
-  return g < ntiles ? g : ntiles;
+static int sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
 }
 
-template <class Pol>
-static cudaError_t launch_stage_pol(int hlld, int stage, const void* tmap_in, const StageArgs& a, cudaStream_t s) {
-  const int ntiles = ((a.nx + TX - 1) / TX) * ((a.ny + TY - 1) / TY);
-  const size_t smem = Smem<Pol>::total;
-  const CUtensorMap& tm = *static_cast<const CUtensorMap*>(tmap_in);
+template <class Pol, bool HLLD, int TY, bool BATCHED>
+static int occupancy() {
+  static int per_sm = -1;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (per_sm < 0) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage_kernel<Pol, 1, HLLD, TY, BATCHED>, Geo<TY>::NT,
+                                                  Smem<Pol, TY>::total);
+    per_sm = nb > 0 ? nb : 1;
+  }
+  return per_sm;
+}
+
+template <class Pol, bool HLLD, int TY, bool BATCHED>
+static void launch_one(int stage, const Batch& b, const Member& m0, int parity, int grid, cudaStream_t s) {
+  const size_t smem = Smem<Pol, TY>::total;
+  if (stage == 1)
+    stage_kernel<Pol, 1, HLLD, TY, BATCHED><<<grid, Geo<TY>::NT, smem, s>>>(m0, b, parity);
+  else
+    stage_kernel<Pol, 2, HLLD, TY, BATCHED><<<grid, Geo<TY>::NT, smem, s>>>(m0, b, parity);
+}
+
+template <class Pol, int TY>
+static int occ_pol_ty(int hlld, bool batched) {
+  if (batched) return hlld ? occupancy<Pol, true, TY, true>() : occupancy<Pol, false, TY, true>();
+  return hlld ? occupancy<Pol, true, TY, false>() : occupancy<Pol, false, TY, false>();
+}
+
+template <class Pol, int TY>
+static cudaError_t launch_stage_pol(int hlld, int stage, const Batch& b, const Member* single, int parity, int grid,
+                                    cudaStream_t s) {
+  if (b.ntiles <= 0) return cudaSuccess;
+  const bool batched = single == nullptr;
+  if (grid <= 0) grid = sm_count() * occ_pol_ty<Pol, TY>(hlld, batched);
+  if (grid > b.ntiles) grid = b.ntiles;
+  static const Member empty = {};
+  const Member& m0 = batched ? empty : *single;
   if (hlld) {
-    if (stage == 1)
-      stage_kernel<Pol, 1, true><<<persistent_grid<Pol, 1, true>(ntiles), NT, smem, s>>>(tm, a);
+    if (batched)
+      launch_one<Pol, true, TY, true>(stage, b, m0, parity, grid, s);
     else
-      stage_kernel<Pol, 2, true><<<persistent_grid<Pol, 2, true>(ntiles), NT, smem, s>>>(tm, a);
+      launch_one<Pol, true, TY, false>(stage, b, m0, parity, grid, s);
   } else {
-    if (stage == 1)
-      stage_kernel<Pol, 1, false><<<persistent_grid<Pol, 1, false>(ntiles), NT, smem, s>>>(tm, a);
+    if (batched)
+      launch_one<Pol, false, TY, true>(stage, b, m0, parity, grid, s);
     else
-      stage_kernel<Pol, 2, false><<<persistent_grid<Pol, 2, false>(ntiles), NT, smem, s>>>(tm, a);
+      launch_one<Pol, false, TY, false>(stage, b, m0, parity, grid, s);
   }
   return cudaGetLastError();
 }
 
-static cudaError_t launch_stage(int precision, int hlld, int stage, const void* tmap_in, const StageArgs& a,
-                                cudaStream_t s) {
+template <class Pol>
+static cudaError_t launch_stage_ty(int hlld, int stage, int ty_idx, const Batch& b, const Member* single, int parity,
+                                   int grid, cudaStream_t s) {
+  return ty_idx == 0 ? launch_stage_pol<Pol, kTileHeights[0]>(hlld, stage, b, single, parity, grid, s)
+                     : launch_stage_pol<Pol, kTileHeights[1]>(hlld, stage, b, single, parity, grid, s);
+}
+
+static cudaError_t launch_stage(int precision, int hlld, int stage, int ty_idx, const Batch& b, const Member* single,
+                                int parity, int grid, cudaStream_t s) {
+  if (ty_idx < 0 || ty_idx >= kNumTileHeights) return cudaErrorInvalidValue;
   switch (precision) {
-    case PREC_FP64: return launch_stage_pol<PolF64>(hlld, stage, tmap_in, a, s);
-    case PREC_FP32: return launch_stage_pol<PolF32>(hlld, stage, tmap_in, a, s);
-    case PREC_MIXED: return launch_stage_pol<PolMixed>(hlld, stage, tmap_in, a, s);
+    case PREC_FP64: return launch_stage_ty<PolF64>(hlld, stage, ty_idx, b, single, parity, grid, s);
+    case PREC_FP32: return launch_stage_ty<PolF32>(hlld, stage, ty_idx, b, single, parity, grid, s);
+    case PREC_MIXED: return launch_stage_ty<PolMixed>(hlld, stage, ty_idx, b, single, parity, grid, s);
     default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class Pol>
+static int occ_pol(int hlld, int ty_idx, bool batched) {
+  return ty_idx == 0 ? occ_pol_ty<Pol, kTileHeights[0]>(hlld, batched)
+                     : occ_pol_ty<Pol, kTileHeights[1]>(hlld, batched);
+}
+
+static int ctas_per_sm(int precision, int hlld, int ty_idx, int batched) {
+  switch (precision) {
+    case PREC_FP64: return occ_pol<PolF64>(hlld, ty_idx, batched != 0);
+    case PREC_FP32: return occ_pol<PolF32>(hlld, ty_idx, batched != 0);
+    default: return occ_pol<PolMixed>(hlld, ty_idx, batched != 0);
+  }
+}
+
+static size_t stage_smem(int precision, int ty_idx) {
+  const bool t8 = ty_idx == 0;
+  switch (precision) {
+    case PREC_FP64: return t8 ? Smem<PolF64, kTileHeights[0]>::total : Smem<PolF64, kTileHeights[1]>::total;
+    case PREC_FP32: return t8 ? Smem<PolF32, kTileHeights[0]>::total : Smem<PolF32, kTileHeights[1]>::total;
+    default: return t8 ? Smem<PolMixed, kTileHeights[0]>::total : Smem<PolMixed, kTileHeights[1]>::total;
   }
 }
 
@@ -105,10 +176,10 @@ static cudaError_t launch_aos_to_soa(int precision, const void* aos, int layout,
   const int g = grid_for((long long)nx * ny);
   if (precision == PREC_FP32)
     aos_to_soa_kernel<float><<<g, NTA, 0, s>>>(static_cast<const float*>(aos), layout, static_cast<float*>(u), plane,
-                                              nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
+                                               nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
   else
     aos_to_soa_kernel<double><<<g, NTA, 0, s>>>(static_cast<const double*>(aos), layout, static_cast<double*>(u),
-                                               plane, nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
+                                                plane, nx, ny, pitch, bc[0], bc[1], bc[2], bc[3]);
   return cudaGetLastError();
 }
 
@@ -118,18 +189,11 @@ static cudaError_t launch_soa_to_aos(int precision, const void* u, long long pla
   const int g = grid_for(n);
   if (precision == PREC_FP32)
     soa_to_aos_kernel<float><<<g, NTA, 0, s>>>(static_cast<const float*>(u), plane, nx, ny, pitch, layout,
-                                              static_cast<float*>(aos));
+                                               static_cast<float*>(aos));
   else
     soa_to_aos_kernel<double><<<g, NTA, 0, s>>>(static_cast<const double*>(u), plane, nx, ny, pitch, layout,
-                                               static_cast<double*>(aos));
+                                                static_cast<double*>(aos));
   return cudaGetLastError();
-}
-
-static void tile(int precision, int* tx, int* ty, size_t* smem) {
-  *tx = TX;
-  *ty = TY;
-  *smem = precision == PREC_FP64 ? Smem<PolF64>::total
-                                 : (precision == PREC_FP32 ? Smem<PolF32>::total : Smem<PolMixed>::total);
 }
 
 }  // namespace PMHD_KNS
@@ -140,9 +204,10 @@ static void tile(int precision, int* tx, int* ty, size_t* smem) {
 #define PMHD_TABLE_FN(n) PMHD_TABLE_FN2(n)
 
 const KernelTable& PMHD_TABLE_FN(PMHD_KNS)() {
-  static const KernelTable t = {PMHD_STR(PMHD_KNS),        PMHD_KNS::init,         PMHD_KNS::launch_stage,
-                                PMHD_KNS::launch_speed,    PMHD_KNS::launch_aos_to_soa, PMHD_KNS::launch_soa_to_aos,
-                                PMHD_KNS::tile};
+  static const KernelTable t = {PMHD_STR(PMHD_KNS),          PMHD_KNS::init,
+                                PMHD_KNS::launch_stage,      PMHD_KNS::ctas_per_sm,
+                                PMHD_KNS::launch_speed,      PMHD_KNS::launch_aos_to_soa,
+                                PMHD_KNS::launch_soa_to_aos, PMHD_KNS::stage_smem};
   return t;
 }
 

@@ -50,8 +50,11 @@ using namespace pmhd;
 namespace {
 
 constexpr size_t kScratchBytes = (size_t)PMHD_NOALLOC_SCRATCH_BYTES;
-constexpr size_t kCtrlBytes = 256;
+constexpr size_t kCtrlBytes = 256;    // control block slot
+constexpr size_t kMemberOff = 256;    // grid descriptor (TMA maps, pointers)
+constexpr size_t kHeadBytes = 2048;   // control block + descriptor
 static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block must fit its slot");
+static_assert(kMemberOff + sizeof(Member) <= kHeadBytes, "grid descriptor must fit its slot");
 
 // The fixed working memory of pmhd_advance_noalloc (see the file comment).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -62,24 +65,6 @@ struct DeviceSetup {
 };
 std::mutex g_mu;
 DeviceSetup g_setup[64];
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
 
 size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -116,23 +101,6 @@ int setup_device(int dev, unsigned char** base) {
   return PMHD_OK;
 }
 
-int make_tmap(const KernelTable& kt, int precision, int nx, int ny, int pitch, long long plane, size_t elem,
-              void* base, CUtensorMap* tm) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) return PMHD_ERR_CUDA;
-  int tx, ty;
-  size_t smem;
-  kt.tile(precision, &tx, &ty, &smem);
-  const cuuint64_t dims[3] = {(cuuint64_t)nx + 4, (cuuint64_t)ny + 4, 9};
-  const cuuint64_t strides[2] = {(cuuint64_t)pitch * elem, (cuuint64_t)plane * elem};
-  const cuuint32_t box[3] = {(cuuint32_t)tx + 4, (cuuint32_t)ty + 4, 9};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(tm, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
-                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? PMHD_OK : PMHD_ERR_CUDA;
-}
-
 }  // namespace
 
 namespace {
@@ -140,7 +108,7 @@ size_t scratch_needed(const pmhd_config* cfg) {
   const size_t elem = cfg->precision == PMHD_FP32 ? 4 : 8;
   const size_t pitch = ((size_t)(cfg->nx + 4) + 15) / 16 * 16;
   const size_t plane = pitch * (size_t)(cfg->ny + 4);
-  return kCtrlBytes + 2 * round256(9 * plane * elem);
+  return kHeadBytes + 2 * round256(9 * plane * elem);
 }
 }  // namespace
 
@@ -164,24 +132,32 @@ extern "C" int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, vo
   const int pitch = ((nx + 4) + 15) / 16 * 16;
   const long long plane = (long long)pitch * (ny + 4);
   Ctrl* dctrl = reinterpret_cast<Ctrl*>(base);
-  void* dU = base + kCtrlBytes;
-  void* dU1 = base + kCtrlBytes + round256(9 * (size_t)plane * elem);
+  Member* dmember = reinterpret_cast<Member*>(base + kMemberOff);
+  void* dU = base + kHeadBytes;
+  void* dU1 = base + kHeadBytes + round256(9 * (size_t)plane * elem);
   const KernelTable& kt = cfg->exact ? kernel_table_exact() : kernel_table_fast();
-  CUtensorMap tmU, tmU1;
-  if ((rc = make_tmap(kt, cfg->precision, nx, ny, pitch, plane, elem, dU, &tmU)) != PMHD_OK) return rc;
-  if ((rc = make_tmap(kt, cfg->precision, nx, ny, pitch, plane, elem, dU1, &tmU1)) != PMHD_OK) return rc;
+  Member hm;
+  std::memset(&hm, 0, sizeof(hm));
+  hm.u = dU;
+  hm.u1 = dU1;
+  hm.ctrl = dctrl;
+  hm.plane = plane;
+  hm.nx = nx;
+  hm.ny = ny;
+  hm.pitch = pitch;
+  set_member_physics(hm, cfg->x_min, cfg->x_max, cfg->y_min, cfg->y_max, cfg->gamma, cfg->hlld_tol, cfg->cfl,
+                     cfg->alpha, cfg->order == PMHD_ORDER_MUSCL ? 1 : 0, cfg->bc, f32);
+  if (!encode_member_tmaps(hm, elem)) return PMHD_ERR_CUDA;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Batch batch;
+  batch.members = dmember;
+  batch.tile_member = nullptr;
+  batch.member_tile0 = nullptr;
+  batch.nmembers = 1;
+  batch.ntiles = ((nx + 31) / 32) * ((ny + kTileHeights[0] - 1) / kTileHeights[0]);
 
   // Values the reference holds in its Real type.
   auto tt = [&](double v) { return f32 ? (double)(float)v : v; };
-  double dx, dy;
-  if (f32) {
-    dx = (double)(((float)cfg->x_max - (float)cfg->x_min) / (float)nx);
-    dy = (double)(((float)cfg->y_max - (float)cfg->y_min) / (float)ny);
-  } else {
-    dx = (cfg->x_max - cfg->x_min) / (double)nx;
-    dy = (cfg->y_max - cfg->y_min) / (double)ny;
-  }
 
   // Control block: everything that must start at zero is rewritten here.
   Ctrl h;
@@ -196,38 +172,18 @@ extern "C" int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, vo
     if ((call) != cudaSuccess) return PMHD_ERR_CUDA; \
   } while (0)
   PMHD_NA(cudaMemcpyAsync(dctrl, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  PMHD_NA(cudaMemcpyAsync(dmember, &hm, sizeof(hm), cudaMemcpyHostToDevice, s));
   PMHD_NA(kt.aos_to_soa(cfg->precision, d_in, PMHD_LAYOUT_INTERIOR, dU, plane, nx, ny, pitch, cfg->bc, s));
   PMHD_NA(kt.speed(cfg->precision, dU, plane, nx, ny, pitch, cfg->gamma, dctrl, 0, s));
 
-  StageArgs a[2];
-  for (int st = 0; st < 2; st++) {
-    StageArgs& x = a[st];
-    x.u_in = st == 0 ? dU : dU1;
-    x.u_out = st == 0 ? dU1 : dU;
-    x.u_old = dU;
-    x.ctrl = dctrl;
-    x.plane = plane;
-    x.nx = nx;
-    x.ny = ny;
-    x.pitch = pitch;
-    x.muscl = cfg->order == PMHD_ORDER_MUSCL ? 1 : 0;
-    for (int k = 0; k < 4; k++) x.bc[k] = cfg->bc[k];
-    x.gamma = cfg->gamma;
-    x.tol = cfg->hlld_tol;
-    x.cfl = tt(cfg->cfl);
-    x.alpha = tt(cfg->alpha);
-    x.dx = dx;
-    x.dy = dy;
-  }
   const int hlld = cfg->solver == PMHD_SOLVER_HLLD ? 1 : 0;
   // Steps are launched in pairs (parity 0 then 1) so the final values land
   // in control slot 0; a step past the stop condition is a no-op.
   auto launch_pairs = [&](long long pairs) -> int {
     for (long long q = 0; q < pairs; q++)
       for (int par = 0; par < 2; par++) {
-        a[0].parity = a[1].parity = par;
-        if (kt.stage(cfg->precision, hlld, 1, &tmU, a[0], s) != cudaSuccess) return PMHD_ERR_CUDA;
-        if (kt.stage(cfg->precision, hlld, 2, &tmU1, a[1], s) != cudaSuccess) return PMHD_ERR_CUDA;
+        if (kt.stage(cfg->precision, hlld, 1, 0, batch, &hm, par, 0, s) != cudaSuccess) return PMHD_ERR_CUDA;
+        if (kt.stage(cfg->precision, hlld, 2, 0, batch, &hm, par, 0, s) != cudaSuccess) return PMHD_ERR_CUDA;
       }
     return PMHD_OK;
   };

@@ -25,36 +25,14 @@
 #include "kernel_api.h"
 #include "pmhd.h"
 #include "problems.h"
+#include "runner.h"
 
 using namespace pmhd;
 
 namespace {
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn get_encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
-
 std::mutex g_init_mu;
 bool g_init_done[64][2];
-
-struct Graph {
-  int steps = 0;
-  cudaGraphExec_t exec = nullptr;
-};
 
 }  // namespace
 
@@ -69,15 +47,17 @@ struct pmhd_solver {
   void* dU1 = nullptr;
   Ctrl* dCtrl = nullptr;
   Ctrl* hCtrl = nullptr;  // pinned mirror
-  CUtensorMap tmU, tmU1;
-  std::vector<Graph> graphs;
+  Member* dMember = nullptr;  // this grid as a one-member batch
+  Member hMember;             // its host copy (passed by value to the kernels)
+  Runner run;
+  bool tuned = false;
+  TuneResult tune_result;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // host view of the run
   double t = 0.0;
   long long steps = 0;
   pmhd_stats stats;
   bool failed = false;
-  double dx_tt = 0, dy_tt = 0, cfl_tt = 0;
 };
 
 namespace {
@@ -93,81 +73,8 @@ bool is_fp32(const pmhd_solver* s) { return s->cfg.precision == PMHD_FP32; }
 // Values the reference computes in its Real type (float for the fp32 build).
 double to_time_type(const pmhd_solver* s, double v) { return is_fp32(s) ? (double)(float)v : v; }
 
-int make_tmap(pmhd_solver* s, void* base, CUtensorMap* tm) {
-  EncodeTiledFn enc = get_encode_fn();
-  if (!enc) return PMHD_ERR_CUDA;
-  int tx, ty;
-  size_t smem;
-  s->kt->tile(s->cfg.precision, &tx, &ty, &smem);
-  const cuuint64_t dims[3] = {(cuuint64_t)s->cfg.nx + 4, (cuuint64_t)s->cfg.ny + 4, 9};
-  const cuuint64_t strides[2] = {(cuuint64_t)s->pitch * s->elem, (cuuint64_t)s->plane * s->elem};
-  const cuuint32_t box[3] = {(cuuint32_t)tx + 4, (cuuint32_t)ty + 4, 9};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(tm, s->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
-                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS ? PMHD_OK : PMHD_ERR_CUDA;
-}
-
-StageArgs stage_args(const pmhd_solver* s, int stage, int parity) {
-  StageArgs a;
-  a.u_in = stage == 1 ? s->dU : s->dU1;
-  a.u_out = stage == 1 ? s->dU1 : s->dU;
-  a.u_old = s->dU;
-  a.ctrl = s->dCtrl;
-  a.plane = s->plane;
-  a.nx = s->cfg.nx;
-  a.ny = s->cfg.ny;
-  a.pitch = s->pitch;
-  a.parity = parity;
-  a.muscl = s->cfg.order == PMHD_ORDER_MUSCL ? 1 : 0;
-  for (int k = 0; k < 4; k++) a.bc[k] = s->cfg.bc[k];
-  a.gamma = s->cfg.gamma;
-  a.tol = s->cfg.hlld_tol;
-  a.cfl = s->cfl_tt;
-  a.alpha = to_time_type(s, s->cfg.alpha);
-  a.dx = s->dx_tt;
-  a.dy = s->dy_tt;
-  return a;
-}
-
-// Enqueues `nsteps` steps (2 stage launches each) starting at parity 0.
-cudaError_t enqueue_steps(pmhd_solver* s, int nsteps) {
-  const int hlld = s->cfg.solver == PMHD_SOLVER_HLLD ? 1 : 0;
-  for (int n = 0; n < nsteps; n++) {
-    const int p = n & 1;
-    StageArgs a1 = stage_args(s, 1, p);
-    cudaError_t e = s->kt->stage(s->cfg.precision, hlld, 1, &s->tmU, a1, s->stream);
-    if (e != cudaSuccess) return e;
-    StageArgs a2 = stage_args(s, 2, p);
-    e = s->kt->stage(s->cfg.precision, hlld, 2, &s->tmU1, a2, s->stream);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
-}
-
 int get_graph(pmhd_solver* s, int nsteps, cudaGraphExec_t* out) {
-  for (auto& g : s->graphs)
-    if (g.steps == nsteps) {
-      *out = g.exec;
-      return PMHD_OK;
-    }
-  cudaGraph_t graph = nullptr;
-  PMHD_CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = enqueue_steps(s, nsteps);
-  cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
-  if (e != cudaSuccess || e2 != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    return PMHD_ERR_CUDA;
-  }
-  Graph g;
-  g.steps = nsteps;
-  e = cudaGraphInstantiate(&g.exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) return PMHD_ERR_CUDA;
-  s->graphs.push_back(g);
-  *out = g.exec;
-  return PMHD_OK;
+  return s->run.graph(nsteps, out) == 0 ? PMHD_OK : PMHD_ERR_CUDA;
 }
 
 int check_args(const pmhd_config* c) {
@@ -295,15 +202,6 @@ int pmhd_create(const pmhd_config* cfg, pmhd_solver** out) {
   s->pitch = ((cfg->nx + 4) + 15) / 16 * 16;
   s->plane = (long long)s->pitch * (cfg->ny + 4);
   const size_t bytes = (size_t)9 * s->plane * s->elem;
-  // Time-type values exactly as the reference computes them in Real.
-  if (is_fp32(s)) {
-    s->dx_tt = (double)(((float)cfg->x_max - (float)cfg->x_min) / (float)cfg->nx);
-    s->dy_tt = (double)(((float)cfg->y_max - (float)cfg->y_min) / (float)cfg->ny);
-  } else {
-    s->dx_tt = (cfg->x_max - cfg->x_min) / (double)cfg->nx;
-    s->dy_tt = (cfg->y_max - cfg->y_min) / (double)cfg->ny;
-  }
-  s->cfl_tt = to_time_type(s, cfg->cfl);
   reset_run(s);
   rc = PMHD_OK;
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) rc = PMHD_ERR_CUDA;
@@ -317,8 +215,37 @@ int pmhd_create(const pmhd_config* cfg, pmhd_solver** out) {
     rc = PMHD_ERR_CUDA;
   if (rc == PMHD_OK && (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess))
     rc = PMHD_ERR_CUDA;
-  if (rc == PMHD_OK) rc = make_tmap(s, s->dU, &s->tmU);
-  if (rc == PMHD_OK) rc = make_tmap(s, s->dU1, &s->tmU1);
+  if (rc == PMHD_OK && cudaMalloc(&s->dMember, sizeof(Member)) != cudaSuccess) rc = PMHD_ERR_NOMEM;
+  if (rc == PMHD_OK) {
+    Member m;
+    std::memset(&m, 0, sizeof(m));
+    m.u = s->dU;
+    m.u1 = s->dU1;
+    m.ctrl = s->dCtrl;
+    m.plane = s->plane;
+    m.nx = cfg->nx;
+    m.ny = cfg->ny;
+    m.pitch = s->pitch;
+    set_member_physics(m, cfg->x_min, cfg->x_max, cfg->y_min, cfg->y_max, cfg->gamma, cfg->hlld_tol, cfg->cfl,
+                       cfg->alpha, cfg->order == PMHD_ORDER_MUSCL ? 1 : 0, cfg->bc, is_fp32(s));
+    if (!encode_member_tmaps(m, s->elem)) rc = PMHD_ERR_CUDA;
+    if (rc == PMHD_OK && cudaMemcpy(s->dMember, &m, sizeof(m), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = PMHD_ERR_CUDA;
+    s->hMember = m;
+    s->run.single = &s->hMember;
+    s->run.kt = s->kt;
+    s->run.precision = cfg->precision;
+    s->run.hlld = cfg->solver == PMHD_SOLVER_HLLD ? 1 : 0;
+    s->run.stream = s->stream;
+    for (int t = 0; t < kNumTileHeights; t++) {
+      Batch& b = s->run.batch[t];
+      b.members = s->dMember;
+      b.tile_member = nullptr;
+      b.member_tile0 = nullptr;
+      b.nmembers = 1;
+      b.ntiles = ((cfg->nx + 31) / 32) * ((cfg->ny + kTileHeights[t] - 1) / kTileHeights[t]);
+    }
+  }
   if (rc == PMHD_OK && cudaStreamSynchronize(s->stream) != cudaSuccess) rc = PMHD_ERR_CUDA;
   if (rc != PMHD_OK) {
     cudaGetLastError();
@@ -333,8 +260,8 @@ int pmhd_destroy(pmhd_solver* s) {
   if (!s) return PMHD_OK;
   cudaSetDevice(s->cfg.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  for (auto& g : s->graphs)
-    if (g.exec) cudaGraphExecDestroy(g.exec);
+  s->run.release();
+  if (s->dMember) cudaFree(s->dMember);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->dU) cudaFree(s->dU);
@@ -432,9 +359,19 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   PMHD_CU(s->kt->speed(s->cfg.precision, s->dU, s->plane, s->cfg.nx, s->cfg.ny, s->pitch, s->cfg.gamma, s->dCtrl,
                        0, s->stream));
   const int big = s->cfg.steps_per_graph;
+  long long tune_steps = 0;
+  if (s->cfg.autotune && !s->tuned && (max_steps < 0 || max_steps >= 32)) {
+    // Live steps timed per kernel variant; identical results for every variant.
+    const int per = 2;
+    PMHD_CU(s->run.tune(per, &s->tune_result));
+    tune_steps = (long long)per * s->tune_result.candidates;
+    s->tuned = true;
+  }
   if (max_steps >= 0) {
     // Known step budget: replay exactly enough steps, then check once.
-    long long left = max_steps + (max_steps & 1);
+    long long left = max_steps - tune_steps;
+    if (left < 0) left = 0;
+    left += left & 1;
     cudaGraphExec_t gb = nullptr, g2 = nullptr;
     if (left >= big) {
       int rc = get_graph(s, big, &gb);
@@ -532,6 +469,15 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   s->stats.steps = s->steps;
   s->stats.status = status;
   s->stats.device_ms = ms;
+  s->stats.tile_height = kTileHeights[s->run.choice.ty_idx];
+  {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device);
+    const int def = sms * s->kt->ctas_per_sm(s->cfg.precision, s->run.hlld, s->run.choice.ty_idx, 0);
+    const int g = s->run.choice.grid > 0 ? s->run.choice.grid : def;
+    const int nt = s->run.batch[s->run.choice.ty_idx].ntiles;
+    s->stats.ctas = g < nt ? g : nt;
+  }
   if (status != PMHD_OK) s->failed = true;
   if (stats) *stats = s->stats;
   return status;

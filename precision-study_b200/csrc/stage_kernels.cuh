@@ -1,15 +1,15 @@
 // stage_kernels.cuh -- the fused SSPRK2 stage kernel and its helpers.
 //
 // One launch performs one SSPRK2 stage of the 2D ideal-MHD + mixed-GLM
-// finite-volume step for the whole grid (reference: the kernel chain
+// finite-volume step for every grid of a batch (reference: the kernel chain
 // bcX/bcY -> fluxX -> fluxY -> rhs -> stage1/stage2 of
 // src/mhd/mhd2d_glm_gpu.cu:141-321, plus speedKernel/rateKernel :171-222
-// for the next step's CFL reduction).  Per CTA and 32 x 8 output tile:
+// for the next step's CFL reduction).  Per 32 x TY output tile:
 //
 //   1. TMA loads the stage input tile with its 2-cell halo, all nine SoA
 //      planes, into shared memory (one 3-D box, no multicast).  CTAs are
-//      persistent (SM count x resident CTAs) and load their next tile while
-//      they compute the current one.
+//      persistent and load their next tile while they compute the current
+//      one.
 //   2. Every tile cell is recovered to primitives once (the reference
 //      recovers each cell up to 8 times, once per stencil use; the result of
 //      a recovery depends only on the cell, so this is bit-identical).
@@ -22,9 +22,10 @@
 //      ghost copies for the boundary conditions) and, in stage 2, the
 //      signal speed of the new state for the next step's CFL max.
 //
-// Time stepping state lives in the device control block (Ctrl); the kernels
-// derive ch, dt and the stop condition from it, so many steps can be
-// replayed from one CUDA graph without returning to the host.
+// Time stepping state lives in each grid's device control block (Ctrl); the
+// kernels derive ch, dt and the stop condition from it, so many steps can be
+// replayed from one CUDA graph without returning to the host, and the grids
+// of a batch advance with their own time steps.
 //
 // Precision policies:
 //   PolF64   storage, recovery, flux and update in binary64
@@ -68,35 +69,40 @@ struct PolMixed {
   static constexpr bool kMixed = true;
 };
 
-#ifndef PMHD_TILE_Y
-#define PMHD_TILE_Y 8
-#endif
-constexpr int TX = 32, TY = PMHD_TILE_Y;  // output tile
-constexpr int HX = TX + 4, HY = TY + 4;   // tile with halo
-constexpr int TC = HX * HY;               // cells per loaded tile
-constexpr int NCELL = TX * TY;            // output cells per tile
-constexpr int NW = NCELL / 32 + 1;        // warps per CTA: one per tile row + one
-constexpr int NT = NW * 32;               // threads per stage CTA (288)
+constexpr int TX = 32;                    // tile width: one warp per tile row
 constexpr int NTA = 256;                  // threads per CTA of the auxiliary kernels
-constexpr int FXN = TY * (TX + 1);        // x-interfaces per tile
-constexpr int GYN = (TY + 1) * TX;        // y-interfaces per tile
 constexpr uint32_t kWaitIters = 1u << 22; // bound on mbarrier polls
-static_assert(TX == 32, "one warp per tile row");
+
+// Geometry of a 32 x TY tile: TY warps own one tile row each, one more warp
+// handles the tile's bottom row of y-interfaces and left column of
+// x-interfaces.
+template <int TY_>
+struct Geo {
+  static constexpr int TY = TY_;
+  static constexpr int HX = TX + 4, HY = TY + 4;  // tile with halo
+  static constexpr int TC = HX * HY;              // cells per loaded tile
+  static constexpr int NW = TY + 1;               // warps per CTA
+  static constexpr int NT = NW * 32;              // threads per CTA
+  static constexpr int FXN = TY * (TX + 1);       // x-interfaces per tile
+  static constexpr int GYN = (TY + 1) * TX;       // y-interfaces per tile
+  static_assert(TY <= 32, "the extra warp covers the left column");
+};
 
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 
-// Per-policy launch tuning, measured on B200 at Orszag-Tang 4096^2 (the
-// stage kernel is issue-bound, so these trade occupancy against registers
-// and shared memory):
+// Per-policy, per-tile-height launch tuning, measured on B200 at Orszag-Tang
+// 4096^2 (the stage kernel is issue-bound, so these trade occupancy against
+// registers and shared memory):
 //   nbuf  input tile buffers: 1 = the next tile's TMA load reuses the buffer
 //         as soon as the current tile is recovered (the update then reads
 //         its own cell from global memory, an L2 hit); 2 = double buffering
 //         (the update reads shared memory);
 //   minb  resident CTAs per SM the register allocation is sized for.
-// fp64: 1 buffer, 2 CTAs (a small spill beats halving the resident warps);
-// fp32: 1 buffer, 3 CTAs; mixed: 2 buffers (its binary64 tile is large),
-// 2 CTAs.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64 override for tuning.
-template <class Pol>
+// 32 x 8 tiles: fp64 1 buffer / 2 CTAs (a small spill beats halving the
+// resident warps), fp32 1 / 3, mixed 2 / 2.  32 x 4 tiles keep about the same
+// threads per SM.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64 override the
+// 32 x 8 values for tuning experiments.
+template <class Pol, int TY>
 struct Tune {
   static constexpr bool r64 = sizeof(typename Pol::R) == 8;
 #ifdef PMHD_NBUF
@@ -104,28 +110,32 @@ struct Tune {
 #else
   static constexpr int nbuf = Pol::kMixed ? 2 : 1;
 #endif
-#if defined(PMHD_MINB_R32) && defined(PMHD_MINB_R64)
-  static constexpr int minb = r64 ? PMHD_MINB_R64 : PMHD_MINB_R32;
-#elif defined(PMHD_MINB_R32)
-  static constexpr int minb = r64 ? 2 : PMHD_MINB_R32;
-#elif defined(PMHD_MINB_R64)
-  static constexpr int minb = r64 ? PMHD_MINB_R64 : (Pol::kMixed ? 2 : 3);
+#ifdef PMHD_MINB_R64
+  static constexpr int minb_r64 = PMHD_MINB_R64;
 #else
-  static constexpr int minb = r64 ? 2 : (Pol::kMixed ? 2 : 3);
+  static constexpr int minb_r64 = 2;
 #endif
+#ifdef PMHD_MINB_R32
+  static constexpr int minb_r32 = PMHD_MINB_R32;
+#else
+  static constexpr int minb_r32 = Pol::kMixed ? 2 : 3;
+#endif
+  static constexpr int minb8 = r64 ? minb_r64 : minb_r32;
+  static constexpr int minb = TY == 8 ? minb8 : (TY == 4 ? (minb8 * 9) / 5 : 1);
 };
 
-template <class Pol>
+template <class Pol, int TY>
 struct Smem {
   using S = typename Pol::S;
   using R = typename Pol::R;
-  static constexpr int NBUF = Tune<Pol>::nbuf;
-  static constexpr size_t u_bytes = sizeof(S) * NVAR * TC;  // TMA box size
-  static constexpr size_t u_stride = align128(u_bytes);      // per buffer
+  using G = Geo<TY>;
+  static constexpr int NBUF = Tune<Pol, TY>::nbuf;
+  static constexpr size_t u_bytes = sizeof(S) * NVAR * G::TC;  // TMA box size
+  static constexpr size_t u_stride = align128(u_bytes);         // per buffer
   static constexpr size_t p_off = u_stride * NBUF;
-  static constexpr size_t fx_off = p_off + align128(sizeof(R) * NVAR * TC);
-  static constexpr size_t gy_off = fx_off + align128(sizeof(R) * NVAR * FXN);
-  static constexpr size_t total = gy_off + align128(sizeof(R) * NVAR * GYN);
+  static constexpr size_t fx_off = p_off + align128(sizeof(R) * NVAR * G::TC);
+  static constexpr size_t gy_off = fx_off + align128(sizeof(R) * NVAR * G::FXN);
+  static constexpr size_t total = gy_off + align128(sizeof(R) * NVAR * G::GYN);
 };
 
 // Primitive recovery of one cell in the storage precision.  PolF64/PolF32
@@ -213,22 +223,22 @@ __device__ __forceinline__ void store_cell(S* u, long long plane, int pitch, int
 
 // Face states and Riemann flux of one interface, always computed in x-normal
 // slot order, from the tile's primitives in shared memory (MUSCL) or its
-// conserved states (first order).  A y-interface is solved exactly as the reference solves it:
-// the stencil is read with the x and y slots of velocity/momentum and field
-// swapped (mhdRotateYToX, mhd_common.hpp:381-391), the x-direction routine
-// runs, and the caller stores the flux back through the same swap
-// (mhdRotateFluxXToY, :395-405).  Reconstruction is per component and the
-// primitive->conserved sums are order-independent, so this equals the
-// reference bit for bit.  One copy of the flux code then serves both
-// directions, which keeps the kernel's hot loop inside the instruction cache.
+// conserved states (first order).  A y-interface is solved exactly as the
+// reference solves it: the stencil is read with the x and y slots of
+// velocity/momentum and field swapped (mhdRotateYToX, mhd_common.hpp:381-391),
+// the x-direction routine runs, and the caller stores the flux back through
+// the same swap (mhdRotateFluxXToY, :395-405).  Reconstruction is per
+// component and the primitive->conserved sums are order-independent, so this
+// equals the reference bit for bit.  One copy of the flux code then serves
+// both directions, which keeps the kernel's hot loop inside the instruction
+// cache.
 //   base   tile index of the cell two steps upwind of the interface
 //   stride 1 (x) or HX (y)
 //   o1/o2  plane offsets of the normal / first tangential velocity slot
 //   o5/o6  plane offsets of the normal / first tangential field slot
-template <class Pol, bool HLLD>
+template <class Pol, bool HLLD, int TC>
 __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, int stride, int o1, int o2, int o5,
-                                         int o6, int muscl,
-                                         typename Pol::R ch, const Phys<typename Pol::R>& ph,
+                                         int o6, int muscl, typename Pol::R ch, const Phys<typename Pol::R>& ph,
                                          typename Pol::R* F) {
   using R = typename Pol::R;
   const int off[NVAR] = {0, o1, o2, 3 * TC, 4 * TC, o5, o6, 7 * TC, 8 * TC};
@@ -257,84 +267,181 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
   return glm_flux<R, 0>(UL, UR, ch, HLLD, F, ph);
 }
 
-template <class Pol, int STAGE, bool HLLD>
-__global__ void __launch_bounds__(NT, Tune<Pol>::minb)
-    stage_kernel(const __grid_constant__ CUtensorMap tmap_in, const StageArgs a) {
-  using S = typename Pol::S;
+// Per-member step values (uniform for all tiles of a member in one launch).
+template <class Pol>
+struct StepVals {
+  typename Pol::R ch;
+  typename Pol::TT t, dt;
+  long long step;
+  bool active;
+  int bad_prev;
+};
+
+// Reads a member's control slot and derives ch, dt and whether it steps.
+template <class Pol, int STAGE>
+__device__ __forceinline__ StepVals<Pol> step_values(const Member& m, int p) {
   using R = typename Pol::R;
   using TT = typename Pol::TT;
-  constexpr int NBUF = Tune<Pol>::nbuf;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  R* sP = reinterpret_cast<R*>(smem_raw + Smem<Pol>::p_off);
-  R* sFx = reinterpret_cast<R*>(smem_raw + Smem<Pol>::fx_off);
-  R* sGy = reinterpret_cast<R*>(smem_raw + Smem<Pol>::gy_off);
-  __shared__ __align__(8) uint64_t bar[NBUF];
-  __shared__ unsigned long long red_speed[NW];
-  __shared__ unsigned red_deg[NW], red_np[NW];
-  auto ubuf = [&](int b) { return reinterpret_cast<S*>(smem_raw + (size_t)b * Smem<Pol>::u_stride); };
-
-  const int tid = threadIdx.x;
-  const bool leader = (blockIdx.x == 0 && tid == 0);
-  Ctrl* c = a.ctrl;
-  const int p = a.parity;
-
-  // ---- step control: identical decision in every thread of the grid -----
+  const Ctrl* c = m.ctrl;
+  StepVals<Pol> v;
   const double t_raw = c->t[p];
-  const long long step = c->step[p];
-  const int bad_prev = (STAGE == 1) ? c->bad2 : c->bad1;
-  const bool active = !c->halted && !c->err && bad_prev == BAD_NONE && (TT)t_raw < (TT)c->t_end &&
-                      step < c->step_limit;
-  if (!active) {
-    if (leader) {  // carry the slot forward so the other parity also stops
-      c->t[p ^ 1] = c->t[p];
-      c->step[p ^ 1] = c->step[p];
-      c->chbits[p ^ 1] = c->chbits[p];
-      if (bad_prev != BAD_NONE || c->err) c->halted = 1;
-    }
-    return;
-  }
-  if (tid == 0) prefetch_tmap(&tmap_in);
-
-  const Phys<R> phR = Phys<R>::make(a.gamma, a.tol);
-  const Phys<S> phS = Phys<S>::make(a.gamma, a.tol);
-  const R ch = vmax((R)__longlong_as_double((long long)c->chbits[p]), (R)1.0e-12);
-  const TT t = (TT)t_raw;
-  const TT dxT = (TT)a.dx, dyT = (TT)a.dy;
+  v.step = c->step[p];
+  v.bad_prev = (STAGE == 1) ? c->bad2 : c->bad1;
+  v.active = !c->halted && !c->err && v.bad_prev == BAD_NONE && (TT)t_raw < (TT)c->t_end && v.step < c->step_limit;
+  v.ch = vmax((R)__longlong_as_double((long long)c->chbits[p]), (R)1.0e-12);
+  v.t = (TT)t_raw;
   // max over cells of max(s_x, ch)/dx + max(s_y, ch)/dy equals ch/dx + ch/dy
   // because ch is the maximum of every s_x and s_y (mhd2d_glm_gpu.cu:485-500).
-  const TT max_rate = (TT)ch / dxT + (TT)ch / dyT;
-  TT dt = (TT)a.cfl / max_rate;
+  const TT max_rate = (TT)v.ch / (TT)m.dx + (TT)v.ch / (TT)m.dy;
+  TT dt = (TT)m.cfl / max_rate;
   const TT t_end = (TT)c->t_end;
-  if (t + dt > t_end) dt = t_end - t;
+  if (v.t + dt > t_end) dt = t_end - v.t;
+  v.dt = dt;
+  return v;
+}
 
-  // ---- persistent loop over tiles, next tile's TMA load in flight ---------
-  // The CTA owns tiles blockIdx.x, blockIdx.x + gridDim.x, ...  As soon as a
-  // tile's cells are recovered into sP, sU is free and the next tile's load
-  // is issued, so the load overlaps this tile's flux and update phases.
-  const int tiles_x = (a.nx + TX - 1) / TX;
-  const int ntiles = tiles_x * ((a.ny + TY - 1) / TY);
-  int tile = blockIdx.x;
+// Work accumulated by a CTA for the member it is currently processing;
+// flushed with one atomic per warp when the member changes and at the end.
+struct MemberAcc {
+  int member;
+  unsigned n_deg, n_np;
+  unsigned long long sp_bits;
+};
+
+template <bool HLLD, int STAGE>
+__device__ __forceinline__ void flush_acc(MemberAcc& acc, const Member* members, int lane, int p) {
+  if (acc.member < 0) return;
+  Ctrl* c = members[acc.member].ctrl;
+  if (HLLD) {
+    const unsigned d = warp_sum_u32(acc.n_deg), np = warp_sum_u32(acc.n_np);
+    if (lane == 0 && d) atomicAdd(&c->degenerate, (unsigned long long)d);
+    if (lane == 0 && np) atomicAdd(&c->nonphysical, (unsigned long long)np);
+  }
+  if (STAGE == 2) {
+    const unsigned long long mbits = warp_max_u64(acc.sp_bits);
+    if (lane == 0 && mbits) atomicMax(&c->chbits[p ^ 1], mbits);
+  }
+  acc.n_deg = acc.n_np = 0;
+  acc.sp_bits = 0;
+}
+
+// The member's once-per-launch control updates, done by the thread that
+// processes (or skips) the member's first tile.
+template <class Pol, int STAGE>
+__device__ __forceinline__ void member_bookkeeping(const Member& m, const StepVals<Pol>& v, int p) {
+  Ctrl* c = m.ctrl;
+  if (!v.active) {  // carry the slot forward so the other parity also stops
+    c->t[p ^ 1] = c->t[p];
+    c->step[p ^ 1] = c->step[p];
+    c->chbits[p ^ 1] = c->chbits[p];
+    if (v.bad_prev != BAD_NONE || c->err) c->halted = 1;
+    return;
+  }
+  atomicAdd(&c->active_stage_launches, 1ull);
+  if (STAGE == 1) {
+    c->chbits[p ^ 1] = 0ull;  // stage 2 of this step accumulates into it
+  } else {
+    c->t[p ^ 1] = (double)(v.t + v.dt);
+    c->step[p ^ 1] = v.step + 1;
+    c->last_ch = (double)v.ch;
+    c->last_dt = (double)v.dt;
+  }
+}
+
+// Whether a member steps in this launch (step_values without the arithmetic).
+template <class Pol, int STAGE>
+__device__ __forceinline__ bool member_active(const Member& m, int p) {
+  using TT = typename Pol::TT;
+  const Ctrl* c = m.ctrl;
+  const int bad_prev = (STAGE == 1) ? c->bad2 : c->bad1;
+  return !c->halted && !c->err && bad_prev == BAD_NONE && (TT)c->t[p] < (TT)c->t_end && c->step[p] < c->step_limit;
+}
+
+// BATCHED = false: one grid, passed by value as a kernel parameter (its
+// scalars are then constant-bank operands and its TMA descriptors live in
+// parameter space); `b` only supplies the tile count.  BATCHED = true: the
+// members of `b`, read from device memory per tile.
+template <class Pol, int STAGE, bool HLLD, int TY, bool BATCHED>
+__global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
+    stage_kernel(const __grid_constant__ Member m0, const Batch b, const int p) {
+  using S = typename Pol::S;
+  using R = typename Pol::R;
+  using G = Geo<TY>;
+  constexpr int HX = G::HX, TC = G::TC, NT = G::NT, FXN = G::FXN, GYN = G::GYN;
+  constexpr int NBUF = Tune<Pol, TY>::nbuf;
+  constexpr int TI = kTileHeights[0] == TY ? 0 : 1;  // index into Member::tm
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* sP = reinterpret_cast<R*>(smem_raw + Smem<Pol, TY>::p_off);
+  R* sFx = reinterpret_cast<R*>(smem_raw + Smem<Pol, TY>::fx_off);
+  R* sGy = reinterpret_cast<R*>(smem_raw + Smem<Pol, TY>::gy_off);
+  __shared__ __align__(8) uint64_t bar[NBUF];
+  auto ubuf = [&](int k) { return reinterpret_cast<S*>(smem_raw + (size_t)k * Smem<Pol, TY>::u_stride); };
+
+  const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  unsigned n_deg = 0, n_np = 0;
-  unsigned long long sp_bits = 0;
-  const S* u_in = static_cast<const S*>(a.u_in);
+  auto member_of = [&](int t) { return BATCHED ? b.tile_member[t] : 0; };
+  auto tile0_of = [&](int mi) { return BATCHED ? b.member_tile0[mi] : 0; };
+  auto member = [&](int mi) -> const Member& { return BATCHED ? b.members[mi] : m0; };
+
+  // One grid that does not step this launch: nothing to load.
+  if (!BATCHED && !member_active<Pol, STAGE>(m0, p)) {
+    if (blockIdx.x == 0 && tid == 0) member_bookkeeping<Pol, STAGE>(m0, step_values<Pol, STAGE>(m0, p), p);
+    return;
+  }
+
+  // Next tile of this CTA (stride gridDim.x) whose member steps; members
+  // that do not step get their bookkeeping from whoever meets their tile 0.
+  auto next_active = [&](int t) {
+    if constexpr (BATCHED) {
+      for (; t < b.ntiles; t += gridDim.x) {
+        const int mi = member_of(t);
+        const Member& mm = b.members[mi];
+        if (member_active<Pol, STAGE>(mm, p)) return t;
+        if (t == tile0_of(mi) && tid == 0) member_bookkeeping<Pol, STAGE>(mm, step_values<Pol, STAGE>(mm, p), p);
+      }
+      return b.ntiles;
+    } else {
+      return t < b.ntiles ? t : b.ntiles;
+    }
+  };
+  auto issue = [&](int t, int k) {
+    const int mi = member_of(t);
+    const Member& mm = member(mi);
+    const int lt = t - tile0_of(mi);
+    const int tiles_x = (mm.nx + TX - 1) / TX;
+    mbar_arrive_expect_tx(&bar[k], (uint32_t)Smem<Pol, TY>::u_bytes);
+    tma_load_3d(ubuf(k), &mm.tm[TI][STAGE - 1], &bar[k], (lt % tiles_x) * TX, (lt / tiles_x) * TY, 0);
+  };
+
   if (tid == 0) {
-    for (int b = 0; b < NBUF; b++) mbar_init(&bar[b], 1);
+    for (int k = 0; k < NBUF; k++) mbar_init(&bar[k], 1);
     fence_barrier_init();
   }
   __syncthreads();
-  if (tid == 0 && tile < ntiles) {
-    mbar_arrive_expect_tx(&bar[0], (uint32_t)Smem<Pol>::u_bytes);
-    tma_load_3d(ubuf(0), &tmap_in, &bar[0], (tile % tiles_x) * TX, (tile / tiles_x) * TY, 0);
-  }
-  for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {
-    const int i0 = (tile % tiles_x) * TX, j0 = (tile / tiles_x) * TY;
+  int tile = next_active(blockIdx.x);
+  if (tid == 0 && tile < b.ntiles) issue(tile, 0);
+  MemberAcc acc = {-1, 0, 0, 0ull};
+  StepVals<Pol> v = step_values<Pol, STAGE>(member(BATCHED ? (tile < b.ntiles ? member_of(tile) : 0) : 0), p);
+
+  for (int it = 0; tile < b.ntiles; it++) {
+    const int mi = member_of(tile);
+    const Member& m = member(mi);
+    if (mi != acc.member) {
+      flush_acc<HLLD, STAGE>(acc, BATCHED ? b.members : &m0, lane, p);
+      acc.member = mi;
+      if (BATCHED) v = step_values<Pol, STAGE>(m, p);
+    }
+    const int lt = tile - tile0_of(mi);
+    const int tiles_x = (m.nx + TX - 1) / TX;
+    const int i0 = (lt % tiles_x) * TX, j0 = (lt / tiles_x) * TY;
+    const Phys<R> phR = Phys<R>::make(m.gamma, m.tol);
+    const Phys<S> phS = Phys<S>::make(m.gamma, m.tol);
     const int cb = it % NBUF;                        // buffer of this tile
     const uint32_t par = (uint32_t)(it / NBUF) & 1;  // its mbarrier phase
     S* sU = ubuf(cb);
     const bool got = __syncthreads_and(mbar_wait_bounded(&bar[cb], par, kWaitIters));
     if (!got) {
-      if (tid == 0) atomicExch(&c->err, (int)DERR_TMA_TIMEOUT);
+      if (tid == 0) atomicExch(&m.ctrl->err, (int)DERR_TMA_TIMEOUT);
       mbar_wait_bounded(&bar[cb], par, kWaitIters);  // let the copy land before leaving
       return;
     }
@@ -347,7 +454,7 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
       S U9[NVAR], P9[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) U9[k] = sU[k * TC + q];
-      if (a.muscl) {
+      if (m.muscl) {
         recover_cell<Pol>(U9, P9, phS);
       } else {
 #pragma unroll
@@ -357,13 +464,12 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
       for (int k = 0; k < NVAR; k++) sP[k * TC + q] = (R)P9[k];
     }
     __syncthreads();
-    // The next tile goes into the buffer no thread reads any more: this
-    // one (just recovered) or, double-buffered, the previous tile's.
-    if (tid == 0 && tile + (int)gridDim.x < ntiles) {
-      const int nt = tile + gridDim.x, nb = (it + 1) % NBUF;
+    // The next tile goes into the buffer no thread reads any more: this one
+    // (just recovered) or, double-buffered, the previous tile's.
+    const int next = next_active(tile + gridDim.x);
+    if (tid == 0 && next < b.ntiles) {
       fence_proxy_async_smem();  // order earlier reads of that buffer before the async overwrite
-      mbar_arrive_expect_tx(&bar[nb], (uint32_t)Smem<Pol>::u_bytes);
-      tma_load_3d(ubuf(nb), &tmap_in, &bar[nb], (nt % tiles_x) * TX, (nt / tiles_x) * TY, 0);
+      issue(next, (it + 1) % NBUF);
     }
 
     // ---- interface fluxes --------------------------------------------------
@@ -388,14 +494,14 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
       }
       // x: interface between cells (i0+fx-1, j0+fy) and (i0+fx, j0+fy)
       // y: interface between cells (i0+fx, j0+fy-1) and (i0+fx, j0+fy)
-      const bool valid = axis ? (j0 + fy <= a.ny && i0 + fx < a.nx) : (i0 + fx <= a.nx && j0 + fy < a.ny);
+      const bool valid = axis ? (j0 + fy <= m.ny && i0 + fx < m.nx) : (i0 + fx <= m.nx && j0 + fy < m.ny);
       if (!valid) continue;
       const int base = axis ? fy * HX + fx + 2 : (fy + 2) * HX + fx;
       const int stride = axis ? HX : 1;
       const int o1 = (axis ? 2 : 1) * TC, o2 = (axis ? 1 : 2) * TC;
       const int o5 = (axis ? 6 : 5) * TC, o6 = (axis ? 5 : 6) * TC;
       R F[NVAR];
-      const int st = face_flux<Pol, HLLD>(sP, base, stride, o1, o2, o5, o6, a.muscl, ch, phR, F);
+      const int st = face_flux<Pol, HLLD, TC>(sP, base, stride, o1, o2, o5, o6, m.muscl, v.ch, phR, F);
       R* out = axis ? sGy : sFx;
       const int n_out = axis ? GYN : FXN;
       const int item = axis ? fy * TX + fx : fy * (TX + 1) + fx;
@@ -410,8 +516,8 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
       out[7 * n_out + item] = F[7];
       out[8 * n_out + item] = F[8];
       if (HLLD && ((axis ? fy : fx) >= 1 || (axis ? j0 : i0) == 0)) {
-        n_deg += (st == HLLD_FALLBACK_DEGENERATE);
-        n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
+        acc.n_deg += (st == HLLD_FALLBACK_DEGENERATE);
+        acc.n_np += (st == HLLD_FALLBACK_NONPHYSICAL);
       }
     }
     __syncthreads();
@@ -419,42 +525,46 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
     // ---- divergence, update, checks, store, next-step speed ---------------
     const int tx = lane, ty = warp;
     const int gi = i0 + tx, gj = j0 + ty;
-    if (warp < TY && gi < a.nx && gj < a.ny) {
-      const size_t gidx = (size_t)(gj + GHOST) * a.pitch + (gi + GHOST);
+    if (warp < TY && gi < m.nx && gj < m.ny) {
+      const size_t gidx = (size_t)(gj + GHOST) * m.pitch + (gi + GHOST);
+      const int lc = (ty + 2) * HX + tx + 2;
+      const S* u_in = static_cast<const S*>(STAGE == 1 ? m.u : m.u1);
+      S* u_out = static_cast<S*>(STAGE == 1 ? m.u1 : m.u);
       S Un[NVAR];
       if constexpr (!Pol::kMixed) {
         // Reference order (mhd2d_glm_gpu.cu:282-285, :299, :316-317).
-        const R damping = ch / vmax((R)a.alpha, (R)1.0e-12);
+        const R damping = v.ch / vmax((R)m.alpha, (R)1.0e-12);
+        const R dxR = (R)m.dx, dyR = (R)m.dy, dtR = (R)v.dt;
 #pragma unroll
         for (int k = 0; k < NVAR; k++) {
-          const R uin = NBUF == 2 ? sU[k * TC + (ty + 2) * HX + tx + 2] : u_in[(size_t)k * a.plane + gidx];
-          R rhs = -(sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx]) / (R)dxT -
-                  (sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx]) / (R)dyT;
+          const R uin = NBUF == 2 ? sU[k * TC + lc] : u_in[(size_t)k * m.plane + gidx];
+          R rhs = -(sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx]) / dxR -
+                  (sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx]) / dyR;
           if (k == PSI) rhs -= damping * uin;
           if (STAGE == 1) {
-            Un[k] = uin + (R)dt * rhs;
+            Un[k] = uin + dtR * rhs;
           } else {
-            const S uold = static_cast<const S*>(a.u_old)[(size_t)k * a.plane + gidx];
-            Un[k] = (R)0.5 * uold + (R)0.5 * (uin + (R)dt * rhs);
+            const S uold = static_cast<const S*>(m.u)[(size_t)k * m.plane + gidx];
+            Un[k] = (R)0.5 * uold + (R)0.5 * (uin + dtR * rhs);
           }
         }
       } else {
         // Binary32 fluxes and their differences, binary64 scaling and
         // accumulation.
-        const double damping = (double)ch / fmax(a.alpha, 1.0e-12);
-        const double inv_dx = 1.0 / a.dx, inv_dy = 1.0 / a.dy;
+        const double damping = (double)v.ch / fmax(m.alpha, 1.0e-12);
+        const double inv_dx = 1.0 / m.dx, inv_dy = 1.0 / m.dy;
 #pragma unroll
         for (int k = 0; k < NVAR; k++) {
-          const double uin = NBUF == 2 ? sU[k * TC + (ty + 2) * HX + tx + 2] : u_in[(size_t)k * a.plane + gidx];
+          const double uin = NBUF == 2 ? sU[k * TC + lc] : u_in[(size_t)k * m.plane + gidx];
           const float dfx = sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx];
           const float dgy = sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx];
           double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
           if (k == PSI) rhs -= damping * uin;
           if (STAGE == 1) {
-            Un[k] = uin + (double)dt * rhs;
+            Un[k] = uin + (double)v.dt * rhs;
           } else {
-            const double uold = static_cast<const double*>(a.u_old)[(size_t)k * a.plane + gidx];
-            Un[k] = 0.5 * uold + 0.5 * (uin + (double)dt * rhs);
+            const double uold = static_cast<const double*>(m.u)[(size_t)k * m.plane + gidx];
+            Un[k] = 0.5 * uold + 0.5 * (uin + (double)v.dt * rhs);
           }
         }
       }
@@ -463,62 +573,22 @@ __global__ void __launch_bounds__(NT, Tune<Pol>::minb)
       S P9[NVAR];
       recover_cell<Pol>(Un, P9, phS);
       if (!(Un[RHO] > rho_floor<S>()) || !prim9_usable<S>(P9)) {
-        atomicMin(STAGE == 1 ? &c->bad1 : &c->bad2, gj * a.nx + gi);
-        c->bad_step = step;
+        atomicMin(STAGE == 1 ? &m.ctrl->bad1 : &m.ctrl->bad2, gj * m.nx + gi);
+        m.ctrl->bad_step = v.step;
       }
-      store_cell<S>(static_cast<S*>(a.u_out), a.plane, a.pitch, gi, gj, a.nx, a.ny, a.bc, Un);
+      store_cell<S>(u_out, m.plane, m.pitch, gi, gj, m.nx, m.ny, m.bc, Un);
       if (STAGE == 2) {
         R Pr[NVAR];
 #pragma unroll
         for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
-        const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, phR));
-        sp_bits = b > sp_bits ? b : sp_bits;
+        const unsigned long long sb = speed_bits((double)cell_speed<R>(Pr, phR));
+        acc.sp_bits = sb > acc.sp_bits ? sb : acc.sp_bits;
       }
     }
+    if (lt == 0 && tid == 0) member_bookkeeping<Pol, STAGE>(m, v, p);
+    tile = next;
   }
-
-  // ---- block reductions, one atomic per CTA ----------------------------------
-  if (HLLD) {
-    const unsigned d = warp_sum_u32(n_deg), np = warp_sum_u32(n_np);
-    if (lane == 0) {
-      red_deg[warp] = d;
-      red_np[warp] = np;
-    }
-  }
-  if (STAGE == 2) {
-    const unsigned long long m = warp_max_u64(sp_bits);
-    if (lane == 0) red_speed[warp] = m;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    if (HLLD) {
-      unsigned d = 0, np = 0;
-#pragma unroll
-      for (int w = 0; w < NW; w++) {
-        d += red_deg[w];
-        np += red_np[w];
-      }
-      if (d) atomicAdd(&c->degenerate, (unsigned long long)d);
-      if (np) atomicAdd(&c->nonphysical, (unsigned long long)np);
-    }
-    if (STAGE == 2) {
-      unsigned long long m = 0;
-#pragma unroll
-      for (int w = 0; w < NW; w++) m = red_speed[w] > m ? red_speed[w] : m;
-      if (m) atomicMax(&c->chbits[p ^ 1], m);
-    }
-  }
-  if (leader) {
-    atomicAdd(&c->active_stage_launches, 1ull);
-    if (STAGE == 1) {
-      c->chbits[p ^ 1] = 0ull;  // stage 2 of this step accumulates into it
-    } else {
-      c->t[p ^ 1] = (double)(t + dt);
-      c->step[p ^ 1] = step + 1;
-      c->last_ch = (double)ch;
-      c->last_dt = (double)dt;
-    }
-  }
+  flush_acc<HLLD, STAGE>(acc, BATCHED ? b.members : &m0, lane, p);
 }
 
 // ---- initial CFL speed: max over interior cells into chbits[slot] ----------

@@ -57,7 +57,7 @@ class Config(ctypes.Structure):
         ("order", ctypes.c_int), ("solver", ctypes.c_int),
         ("precision", ctypes.c_int), ("exact", ctypes.c_int),
         ("bc", ctypes.c_int * 4), ("device", ctypes.c_int),
-        ("steps_per_graph", ctypes.c_int),
+        ("steps_per_graph", ctypes.c_int), ("autotune", ctypes.c_int),
     ]
 
 
@@ -69,7 +69,7 @@ class Stats(ctypes.Structure):
         ("degenerate", ctypes.c_ulonglong), ("nonphysical", ctypes.c_ulonglong),
         ("status", ctypes.c_int), ("bad_i", ctypes.c_int), ("bad_j", ctypes.c_int),
         ("bad_step", ctypes.c_longlong), ("kernel_launches", ctypes.c_ulonglong),
-        ("device_ms", ctypes.c_double),
+        ("device_ms", ctypes.c_double), ("tile_height", ctypes.c_int), ("ctas", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -140,7 +140,7 @@ def problem_state(problem, params=None, **cfg_kwargs):
 
 def make_config(nx=128, ny=128, precision="fp64", exact=False, order="muscl", solver="hlld", cfl=0.25,
                 alpha=0.18, gamma=5.0 / 3.0, hlld_tol=1e-4, domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0),
-                device=0, steps_per_graph=0):
+                device=0, steps_per_graph=0, autotune=False):
     c = default_config()
     c.nx, c.ny = nx, ny
     c.x_min, c.x_max, c.y_min, c.y_max = domain
@@ -153,6 +153,7 @@ def make_config(nx=128, ny=128, precision="fp64", exact=False, order="muscl", so
         c.bc[k] = bc[k]
     c.device = device
     c.steps_per_graph = steps_per_graph
+    c.autotune = int(bool(autotune))
     return c
 
 
@@ -166,10 +167,10 @@ class Solver:
 
     def __init__(self, nx=128, ny=128, precision="fp64", exact=False, order="muscl",
                  solver="hlld", cfl=0.25, alpha=0.18, gamma=5.0 / 3.0, hlld_tol=1e-4,
-                 domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0), device=0, steps_per_graph=0):
+                 domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0), device=0, steps_per_graph=0, autotune=False):
         L = load()
         c = make_config(nx, ny, precision, exact, order, solver, cfl, alpha, gamma, hlld_tol, domain, bc,
-                        device, steps_per_graph)
+                        device, steps_per_graph, autotune)
         self.cfg = c
         self.dtype = np.float32 if c.precision == FP32 else np.float64
         h = ctypes.c_void_p()
