@@ -193,6 +193,41 @@ def time_precision(pmhd, precision, n, warmup, steps, device, sampler=None):
     return s, st, launches
 
 
+def bench_ensemble(pmhd, nmem, seed, prec, W, K, device, barrier, max_over_ranks, world):
+    """Zone-cycles/s of the seeded uneven ensemble (square grids from
+    {64,128,256,512}, half Orszag-Tang with scaled field, half Brio-Wu bands
+    at a drawn slope) advanced by shared persistent launches, beside the same
+    members advanced one grid at a time by the single-grid path."""
+    ms_desc = pmhd.describe_ensemble(nmem, seed)
+    e = pmhd.Ensemble(ms_desc, precision=prec, autotune=True, device=device)
+    # Warm-up includes the autotuner (it needs a budget of >= 32 steps).
+    e.advance(max_steps=max(32, W))
+    barrier()
+    tot = e.advance(max_steps=K)
+    barrier()
+    ms = max_over_ranks(tot.device_ms)
+    cells = sum(m.nx * m.ny for m in ms_desc)
+    out = {"value": world * tot.zone_cycles / (ms / 1e3), "unit": UNIT, "members": nmem, "seed": seed,
+           "cells": cells, "steps": K, "warmup_steps": max(32, W), "ms_per_step": ms / K,
+           "tile_height": tot.tile_height, "ctas": tot.ctas, "gpu_launches": tot.kernel_launches,
+           "status": tot.status,
+           "sizes": {str(s): sum(1 for m in ms_desc if m.nx == s) for s in (64, 128, 256, 512)}}
+    e.close()
+    # One grid at a time: the same members through pmhd_advance (same kernels,
+    # one launch sequence per grid), device time summed.
+    tot_ms, zc = 0.0, 0
+    for d in ms_desc:
+        with pmhd.Solver(nx=d.nx, ny=d.ny, gamma=d.gamma, bc=tuple(d.bc), precision=prec, device=device) as s:
+            s.init_problem(d.problem, list(d.params[:d.nparams]))
+            s.advance(max_steps=max(32, W))
+            st = s.advance(max_steps=K)
+            tot_ms += st.device_ms
+            zc += st.zone_cycles
+    out["one_grid_at_a_time"] = {"value": world * zc / (max_over_ranks(tot_ms) / 1e3), "unit": UNIT}
+    out["speedup_vs_one_grid_at_a_time"] = out["value"] / out["one_grid_at_a_time"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,6 +242,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=1024, help="grid of one reference CPU sample")
     ap.add_argument("--ref-instances", type=int, default=16, help="max concurrent reference processes")
     ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
+    ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
+    ap.add_argument("--ensemble-seed", type=int, default=2024)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -310,6 +347,12 @@ def main():
                "note": "one C-ABI run per timed region: pmhd_set_state from pinned host AoS, "
                        f"pmhd_advance of {K} steps, pmhd_get_state to pinned host AoS"}
 
+    # ---- ensemble: uneven grids in one persistent launch per stage -----------
+    ens = None
+    if args.ensemble > 0:
+        ens = bench_ensemble(pmhd, args.ensemble, args.ensemble_seed, prec, W, K, local, barrier, max_over_ranks,
+                             world)
+
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -336,6 +379,8 @@ def main():
             "cpu_baseline": cpu, "steps_run": {"t": st.t, "steps": st.steps},
         }
         line.update(extra)
+        if ens is not None:
+            line["ensemble"] = ens
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -67,7 +67,8 @@ typedef enum {
   PMHD_PROBLEM_ORSZAG_TANG = 0, /* mhd2d_glm_gpu.cu:443-451, unit periodic box        */
   PMHD_PROBLEM_KH_REF = 1,      /* the reference's doubly periodic double shear layer */
   PMHD_PROBLEM_KH_REFLECT = 2,  /* single shear layer, x periodic, y reflecting       */
-  PMHD_PROBLEM_BRIO_WU_2D = 3   /* Brio-Wu Riemann problem, interface rotated         */
+  PMHD_PROBLEM_BRIO_WU_2D = 3,  /* Brio-Wu Riemann problem, interface rotated         */
+  PMHD_PROBLEM_BRIO_WU_TORUS = 4 /* Brio-Wu states in bands of slope k/m, periodic    */
 } pmhd_problem;
 typedef enum { PMHD_LAYOUT_INTERIOR = 0, PMHD_LAYOUT_GHOSTED = 1 } pmhd_layout;
 
@@ -112,6 +113,8 @@ typedef struct {
                                        CUDA events on the handle's stream     */
   int tile_height;                  /* stage-kernel tile height in use (8, 4)  */
   int ctas;                         /* persistent CTAs per stage launch        */
+  unsigned long long zone_cycles;   /* cells x steps of the last advance
+                                       (summed over ensemble members)         */
 } pmhd_stats;
 
 typedef struct pmhd_solver pmhd_solver;
@@ -130,6 +133,11 @@ int pmhd_destroy(pmhd_solver* s);
  *   ORSZAG_TANG:   params[0] = field amplitude factor B0 (1 = reference)
  *   KH_REFLECT:    params[0] = shear-layer width (0.05), params[1] = Bx (0.1)
  *   BRIO_WU_2D:    params[0] = interface angle in radians (0)
+ *   BRIO_WU_TORUS: params[0] = k, params[1] = m (integers >= 0, not both 0;
+ *                  default 1, 2): the interface normal is (m/Lx, k/Ly), the
+ *                  Brio-Wu left state fills half of each of the bands of one
+ *                  period m x + k y along it, so the pattern is periodic on the
+ *                  box and every band edge is a Brio-Wu (or mirrored) jump
  * gamma, domain and boundary kinds are taken from the handle's config. */
 int pmhd_init_problem(pmhd_solver* s, int problem, const double* params, int nparams);
 
@@ -175,6 +183,52 @@ const char* pmhd_strerror(int status);
 
 /* Copies the configuration a handle was created with. */
 int pmhd_get_config(const pmhd_solver* s, pmhd_config* cfg);
+
+/* ---- Ensembles: many independent grids advanced by the same launches -------
+ * No counterpart in the reference (it runs one grid per process).  Every
+ * member has its own grid size, domain, gamma, boundary kinds, initial
+ * condition and end time, and advances with its own CFL time step; all
+ * members' tiles form one work list of one persistent stage launch per SSPRK2
+ * stage, replayed from CUDA graphs.  The common configuration supplies
+ * precision, exact, order, solver, cfl, alpha, hlld_tol, device,
+ * steps_per_graph and autotune (its nx, ny, domain, gamma and bc are
+ * ignored).  Each member gives the same results as a single pmhd_solver run
+ * of it. */
+typedef struct {
+  int nx, ny;
+  double x_min, x_max, y_min, y_max;
+  double gamma;
+  int bc[4];            /* x low, x high, y low, y high (pmhd_bc)              */
+  int problem;          /* pmhd_problem building the initial state             */
+  int nparams;          /* parameters of that problem (see pmhd_init_problem)  */
+  double params[4];
+  double t_end;         /* the member stops when !(t < t_end)                  */
+} pmhd_member_desc;
+
+typedef struct pmhd_ensemble pmhd_ensemble;
+
+/* Fills out[0..n-1] with the benchmark ensemble: square grids drawn uniformly
+ * from {64, 128, 256, 512}; even members Orszag-Tang with the field scaled by
+ * B0 ~ U[0.5, 1.5] (gamma 5/3, periodic, t_end 0.5), odd members the Brio-Wu
+ * tube (gamma 2, t_end 0.1) with its interface rotated by an angle
+ * ~ U[0, pi/2]; the draws come from splitmix64 seeded with `seed` (three
+ * draws per member: size, amplitude or angle, spare). */
+int pmhd_ensemble_describe_default(int n, unsigned long long seed, pmhd_member_desc* out);
+
+int pmhd_ensemble_create(const pmhd_config* common, const pmhd_member_desc* members, int n, pmhd_ensemble** out);
+
+/* Advances every member until its t_end, or by at most max_steps steps per
+ * member in this call (max_steps < 0: no limit).  total: steps = the largest
+ * member step count, zone_cycles and HLLD counters summed, kernel_launches =
+ * kernels enqueued (stage launches with or without work, CFL reductions),
+ * device_ms, tile_height / ctas of the kernel variant; status = the first
+ * failing member's status (PMHD_OK if none).  Per-member statistics
+ * (pmhd_ensemble_member_stats) count that member's stage launches with work. */
+int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* total);
+
+int pmhd_ensemble_member_stats(const pmhd_ensemble* e, int k, pmhd_stats* st);
+int pmhd_ensemble_get_state(pmhd_ensemble* e, int k, void* host, int layout);
+int pmhd_ensemble_destroy(pmhd_ensemble* e);
 
 /* ---- Allocation-free time loop ----------------------------------------------
  * No counterpart in the reference: its program always cudaMallocs five state

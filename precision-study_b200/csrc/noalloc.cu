@@ -231,6 +231,7 @@ extern "C" int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, vo
     out.nonphysical = r.nonphysical;
   }
   out.kernel_launches = r.active_stage_launches + 1;
+  out.zone_cycles = (unsigned long long)(r.step[0] - step0) * (unsigned long long)nx * ny;
   out.status = status;
   if (stats) *stats = out;
   return status;

@@ -42,6 +42,17 @@ bool init_problem_host(const ProblemGrid& g, int problem, const double* params, 
   const T kh_bx = (T)par(1, 0.1);              // KH_REFLECT parallel field
   const double angle = par(0, 0.0);            // BRIO_WU_2D interface angle
   const T cth = (T)std::cos(angle), sth = (T)std::sin(angle);
+  // BRIO_WU_TORUS: band slope k/m; unit normal and tangent of the bands.
+  const double kb = par(0, 1.0), mb = par(1, 2.0);
+  if (problem == PMHD_PROBLEM_BRIO_WU_TORUS &&
+      (kb < 0 || mb < 0 || kb != std::floor(kb) || mb != std::floor(mb) || kb + mb == 0 || kb > 64 || mb > 64))
+    return false;
+  const double nxb = mb / (g.x_max - g.x_min), nyb = kb / (g.y_max - g.y_min);
+  const double nlen = std::sqrt(nxb * nxb + nyb * nyb);
+  const T bnx = (T)(nxb / nlen), bny = (T)(nyb / nlen);
+  // Band edges at phases 1/(4 n) and 1/2 + 1/(4 n), n = max(nx, ny): on a
+  // square grid with even n no cell centre lies on an edge.
+  const double phase0 = 0.25 / (double)(nx > ny ? nx : ny);
   for (int j = 0; j < nyt; j++) {
     for (int i = 0; i < nxt; i++) {
       const T x = x_min + ((T)(i - G) + (T)0.5) * dx;
@@ -101,6 +112,24 @@ bool init_problem_host(const ProblemGrid& g, int problem, const double* params, 
           P[4] = left ? (T)1.0 : (T)0.1;
           P[5] = bn * cth - bt * sth;
           P[6] = bn * sth + bt * cth;
+          P[7] = (T)0.0;
+          P[8] = (T)0.0;
+          break;
+        }
+        case PMHD_PROBLEM_BRIO_WU_TORUS: {  // mhd1d_cpu.cpp:283-295 states in periodic bands
+          const double xc = g.x_min + ((i - G) + 0.5) * (g.x_max - g.x_min) / nx;
+          const double yc = g.y_min + ((j - G) + 0.5) * (g.y_max - g.y_min) / ny;
+          double phs = mb * (xc - g.x_min) / (g.x_max - g.x_min) + kb * (yc - g.y_min) / (g.y_max - g.y_min) - phase0;
+          phs -= std::floor(phs);
+          const bool left = phs < 0.5;
+          const T bn = (T)0.75, bt = left ? (T)1.0 : (T)-1.0;
+          P[0] = left ? (T)1.0 : (T)0.125;
+          P[1] = (T)0.0;
+          P[2] = (T)0.0;
+          P[3] = (T)0.0;
+          P[4] = left ? (T)1.0 : (T)0.1;
+          P[5] = bn * bnx - bt * bny;
+          P[6] = bn * bny + bt * bnx;
           P[7] = (T)0.0;
           P[8] = (T)0.0;
           break;

@@ -469,6 +469,7 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   s->stats.steps = s->steps;
   s->stats.status = status;
   s->stats.device_ms = ms;
+  s->stats.zone_cycles = (unsigned long long)done_steps * (unsigned long long)s->cfg.nx * s->cfg.ny;
   s->stats.tile_height = kTileHeights[s->run.choice.ty_idx];
   {
     int sms = 0;

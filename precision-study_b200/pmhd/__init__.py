@@ -27,7 +27,7 @@ FP64, FP32, MIXED = 0, 1, 2
 BC_PERIODIC, BC_REFLECT, BC_TRANSMISSIVE = 0, 1, 2
 ORDER_FIRST, ORDER_MUSCL = 0, 1
 SOLVER_HLL, SOLVER_HLLD = 0, 1
-PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D = 0, 1, 2, 3
+PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D, PROBLEM_BRIO_WU_TORUS = 0, 1, 2, 3, 4
 LAYOUT_INTERIOR, LAYOUT_GHOSTED = 0, 1
 
 PRECISIONS = {"fp64": FP64, "fp32": FP32, "mixed": MIXED}
@@ -38,6 +38,8 @@ EXPORTS = (
     "pmhd_set_state", "pmhd_get_state", "pmhd_set_time", "pmhd_advance",
     "pmhd_get_stats", "pmhd_diagnostics", "pmhd_write_dat", "pmhd_dat_filename",
     "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state", "pmhd_advance_noalloc",
+    "pmhd_ensemble_describe_default", "pmhd_ensemble_create", "pmhd_ensemble_advance",
+    "pmhd_ensemble_member_stats", "pmhd_ensemble_get_state", "pmhd_ensemble_destroy",
 )
 
 
@@ -70,10 +72,29 @@ class Stats(ctypes.Structure):
         ("status", ctypes.c_int), ("bad_i", ctypes.c_int), ("bad_j", ctypes.c_int),
         ("bad_step", ctypes.c_longlong), ("kernel_launches", ctypes.c_ulonglong),
         ("device_ms", ctypes.c_double), ("tile_height", ctypes.c_int), ("ctas", ctypes.c_int),
+        ("zone_cycles", ctypes.c_ulonglong),
     ]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class MemberDesc(ctypes.Structure):
+    """pmhd_member_desc: one member of an ensemble."""
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+        ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("bc", ctypes.c_int * 4),
+        ("problem", ctypes.c_int), ("nparams", ctypes.c_int), ("params", ctypes.c_double * 4),
+        ("t_end", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["bc"] = tuple(self.bc)
+        d["params"] = tuple(self.params[:self.nparams])
+        return d
 
 
 _lib = None
@@ -105,6 +126,12 @@ def load():
         "pmhd_get_config": ([vp, P(Config)], i),
         "pmhd_problem_state": ([P(Config), i, P(d), i, vp], i),
         "pmhd_advance_noalloc": ([P(Config), vp, vp, d, ctypes.c_longlong, d, ctypes.c_longlong, vp, P(Stats)], i),
+        "pmhd_ensemble_describe_default": ([i, ctypes.c_ulonglong, P(MemberDesc)], i),
+        "pmhd_ensemble_create": ([P(Config), P(MemberDesc), i, P(vp)], i),
+        "pmhd_ensemble_advance": ([vp, ctypes.c_longlong, P(Stats)], i),
+        "pmhd_ensemble_member_stats": ([vp, i, P(Stats)], i),
+        "pmhd_ensemble_get_state": ([vp, i, vp, i], i),
+        "pmhd_ensemble_destroy": ([vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -247,6 +274,90 @@ class Solver:
         buf = ctypes.create_string_buffer(512)
         _check(load().pmhd_dat_filename(self._h, prob_base.encode(), buf, 512), "pmhd_dat_filename")
         return buf.value.decode()
+
+
+def describe_ensemble(n, seed=0):
+    """The benchmark ensemble (pmhd_ensemble_describe_default): a ctypes
+    array of n MemberDesc; needs no GPU."""
+    arr = (MemberDesc * n)()
+    _check(load().pmhd_ensemble_describe_default(n, seed, arr), "pmhd_ensemble_describe_default")
+    return arr
+
+
+def member(nx, ny, problem=PROBLEM_ORSZAG_TANG, params=(), t_end=0.5, gamma=5.0 / 3.0,
+           domain=(0.0, 1.0, 0.0, 1.0), bc=(0, 0, 0, 0)):
+    """One MemberDesc from keyword arguments."""
+    m = MemberDesc()
+    m.nx, m.ny = nx, ny
+    m.x_min, m.x_max, m.y_min, m.y_max = domain
+    m.gamma = gamma
+    for k in range(4):
+        m.bc[k] = bc[k]
+    m.problem = problem
+    m.nparams = len(params)
+    for k, v in enumerate(params):
+        m.params[k] = v
+    m.t_end = t_end
+    return m
+
+
+class Ensemble:
+    """Many independent grids advanced by the same launches (a pmhd_ensemble
+    handle).  `members` is a sequence (or ctypes array) of MemberDesc; the
+    keyword arguments give the common configuration as for Solver."""
+
+    def __init__(self, members, precision="fp64", exact=False, order="muscl", solver="hlld", cfl=0.25,
+                 alpha=0.18, hlld_tol=1e-4, device=0, steps_per_graph=0, autotune=False):
+        L = load()
+        n = len(members)
+        arr = members if isinstance(members, ctypes.Array) else (MemberDesc * n)(*members)
+        self.members = arr
+        c = make_config(precision=precision, exact=exact, order=order, solver=solver, cfl=cfl, alpha=alpha,
+                        hlld_tol=hlld_tol, device=device, steps_per_graph=steps_per_graph, autotune=autotune)
+        self.cfg = c
+        self.dtype = np.float32 if c.precision == FP32 else np.float64
+        h = ctypes.c_void_p()
+        _check(L.pmhd_ensemble_create(ctypes.byref(c), arr, n, ctypes.byref(h)), "pmhd_ensemble_create")
+        self._h = h
+
+    def __len__(self):
+        return len(self.members)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pmhd_ensemble_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, max_steps=-1, check=True):
+        st = Stats()
+        rc = load().pmhd_ensemble_advance(self._h, max_steps, ctypes.byref(st))
+        if check:
+            _check(rc, "pmhd_ensemble_advance")
+        return st
+
+    def member_stats(self, k):
+        st = Stats()
+        _check(load().pmhd_ensemble_member_stats(self._h, k, ctypes.byref(st)), "pmhd_ensemble_member_stats")
+        return st
+
+    def get_state(self, k, layout=LAYOUT_INTERIOR):
+        m = self.members[k]
+        shape = (m.ny, m.nx, 9) if layout == LAYOUT_INTERIOR else (m.ny + 4, m.nx + 4, 9)
+        out = np.empty(shape, dtype=self.dtype)
+        _check(load().pmhd_ensemble_get_state(self._h, k, out.ctypes.data, layout), "pmhd_ensemble_get_state")
+        return out
 
 
 def relative_l2(ref, other):
