@@ -230,6 +230,32 @@ int pmhd_ensemble_member_stats(const pmhd_ensemble* e, int k, pmhd_stats* st);
 int pmhd_ensemble_get_state(pmhd_ensemble* e, int k, void* host, int layout);
 int pmhd_ensemble_destroy(pmhd_ensemble* e);
 
+/* ---- Learned coarse-grid correction: network building blocks --------------
+ * No counterpart in the reference (its learned part exists only as a plan).
+ * BF16 tensor-core (tcgen05) 3x3 convolutions over device NHWC bf16 images
+ * [batch][h][w][channels], periodic in y and x; weights [c_out][9][c_in],
+ * tap t = (dy+1)*3 + (dx+1), out(y,x) = sum_t W[t] x(y+dy, x+dx) + bias.
+ * Enqueued on `stream` (a cudaStream_t, NULL = default) and synchronised
+ * before returning; all pointers are device pointers, 16-byte aligned.
+ *   PMHD_CONV_GELU:   out0 = z (bf16), out1 = gelu(z) (bf16), (c_in, c_out) = (32, 32)
+ *   PMHD_CONV_LINEAR: out0 = fp32 result, (32, 16)
+ *   PMHD_CONV_DGELU:  backward to the input of a GELU layer: x = the
+ *                     layer's output gradient (c_in = its outputs), weight =
+ *                     its weights transposed to [c_out][9][c_in], z_prev =
+ *                     the previous layer's z; out0 = that z's gradient
+ *                     (bf16); (16, 32) or (32, 32)
+ * PMHD_ERR_UNSUPPORTED for other channel counts, PMHD_ERR_TIMEOUT when a
+ * bounded wait in the kernel expired. */
+typedef enum { PMHD_CONV_GELU = 0, PMHD_CONV_LINEAR = 1, PMHD_CONV_DGELU = 2 } pmhd_conv_mode;
+int pmhd_conv3x3(int mode, const void* x, int batch, int h, int w, int c_in, const void* weight, const float* bias,
+                 int c_out, const void* z_prev, void* out0, void* out1, void* stream);
+
+/* Weight and bias gradients of a 3x3 layer: dweight[co][t][ci] +=
+ * sum_p dz[p][co] x[p + tap t][ci], dbias[co] += sum_p dz[p][co] (dbias may
+ * be NULL); fp32 accumulation.  (c_in, c_out) = (32, 32) or (32, 16). */
+int pmhd_conv3x3_wgrad(const void* x, const void* dz, int batch, int h, int w, int c_in, int c_out, float* dweight,
+                       float* dbias, void* stream);
+
 /* ---- Allocation-free time loop ----------------------------------------------
  * No counterpart in the reference: its program always cudaMallocs five state
  * arrays.  For callers that must not allocate device memory while they run

@@ -1,0 +1,410 @@
+// conv.cu -- BF16 tensor-core (tcgen05, accumulators in tensor memory) 3x3
+// convolutions of the learned coarse-grid correction: forward with bias and
+// GELU, forward linear, backward to the input through the previous layer's
+// GELU, and the weight gradient.  Images are NHWC bf16 tensors
+// [batch][h][w][channels], periodic in y and x (the coarse grids they come
+// from are periodic).  Weights are [c_out][9][c_in] with tap t = (dy+1)*3 +
+// (dx+1): out(y, x) = sum_t W[t] x(y+dy, x+dx) (cross-correlation).
+//
+// Implicit GEMM.  Forward / backward-data: one CTA computes 128 output
+// pixels (M = 128) x c_out channels (N); K = 9 taps x c_in channels.  The
+// CTA gathers the 9 shifted copies of its pixels' input vectors (periodic
+// wrap) into K-major shared-memory tiles, one thread issues 9 * c_in / 16
+// tcgen05.mma, the four warps read the 128 x N accumulator back with
+// tcgen05.ld and run the epilogue.  Weight gradient: D[(t, c_in)][c_out] =
+// sum over pixels of x(p + tap) dz(p)^T, K = pixels, both operands gathered
+// MN-major (channel vectors are contiguous in NHWC), three M = 128 tiles
+// accumulated over 64-pixel chunks, summed over CTAs with fp32 atomics.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "learned/conv.h"
+#include "learned/umma.cuh"
+
+namespace pmhd {
+namespace learned {
+
+namespace {
+
+constexpr uint32_t kWaitPolls = 1u << 22;
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+__device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Bounded wait for the MMA batch; on expiry record the error and wait once
+// more (bounded) so tensor memory is not released under a running MMA.
+__device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t parity, int* err) {
+  bool ok = mbar_wait_bounded(bar, parity, kWaitPolls);
+  ok = __all_sync(0xffffffffu, ok);
+  if (!ok) {
+    if ((threadIdx.x & 31) == 0) atomicExch(err, PMHD_LEARNED_ERR_TIMEOUT);
+    mbar_wait_bounded(bar, parity, kWaitPolls);
+  }
+  return ok;
+}
+
+template <int CG, int CO>
+struct ConvSmem {
+  static constexpr int K = 9 * CG;
+  static constexpr uint32_t kATap = 128u * CG * 2u;  // bytes of one tap tile
+  static constexpr uint32_t kLboA = 128u * 16u;      // K-group stride of A
+  static constexpr uint32_t kBytesB = (uint32_t)CO * K * 2u;
+  static constexpr uint32_t kLboB = (uint32_t)CO * 16u;
+  static constexpr uint32_t kOffB = 9u * kATap;
+  static constexpr uint32_t kOffBar = kOffB + kBytesB;
+  static constexpr uint32_t kBytes = kOffBar + 16u;
+};
+
+// EPI: CONV_GELU   out0 = z (bf16), out1 = gelu(z) (bf16), z = acc + bias
+//      CONV_LINEAR out0 = acc + bias (fp32)
+//      CONV_DGELU  out0 = acc * gelu'(zprev) (bf16); taps mirrored (the
+//                  transposed convolution of the backward pass)
+template <int CG, int CO, int EPI>
+__global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __restrict__ x,
+                                                      const __nv_bfloat16* __restrict__ wt,
+                                                      const float* __restrict__ bias,
+                                                      const __nv_bfloat16* __restrict__ zprev, int batch, int h,
+                                                      int w, void* __restrict__ out0, void* __restrict__ out1,
+                                                      int* __restrict__ err) {
+  using S = ConvSmem<CG, CO>;
+  constexpr uint32_t kCols = umma::tmem_cols(CO);
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + S::kOffB;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const long long P = (long long)batch * h * w;
+  const long long p0 = (long long)blockIdx.x * 128;
+
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  // B operand: weights, row n, K-groups of 8 (16-byte vectors).
+  for (int c = tid; c < CO * (S::K / 8); c += 128) {
+    const int n = c / (S::K / 8), g = c - n * (S::K / 8);
+    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * S::K + g * 8);
+    *reinterpret_cast<uint4*>(sB + n * 16 + g * S::kLboB) = v;
+  }
+  // A operand: for each tap, the 128 pixels' shifted input vectors.
+  for (int c = tid; c < 9 * 128 * (CG / 8); c += 128) {
+    const int g = c % (CG / 8);
+    const int m = (c / (CG / 8)) % 128;
+    const int t = c / (128 * (CG / 8));
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    const long long p = p0 + m;
+    if (p < P) {
+      const int x0 = (int)(p % w);
+      const long long r = p / w;
+      const int y0 = (int)(r % h);
+      const long long b = r / h;
+      int dy = t / 3 - 1, dx = t % 3 - 1;
+      if (EPI == CONV_DGELU) {
+        dy = -dy;
+        dx = -dx;
+      }
+      const int yy = wrap(y0 + dy, h), xx = wrap(x0 + dx, w);
+      v = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CG + g * 8);
+    }
+    *reinterpret_cast<uint4*>(sA + t * S::kATap + m * 16 + g * S::kLboA) = v;
+  }
+  fence_proxy_async_smem();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {
+    constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll 1
+    for (int t = 0; t < 9; t++)
+#pragma unroll
+      for (int kc = 0; kc < CG / 16; kc++) {
+        const uint64_t da = umma::desc(a0 + t * S::kATap + kc * 2 * S::kLboA, S::kLboA, 128);
+        const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * S::kLboB, S::kLboB, 128);
+        umma::mma_bf16(tmem, da, db, idesc, (t | kc) ? 1u : 0u);
+      }
+    umma::commit(bar);
+  }
+  __syncwarp();
+  const bool ok = wait_mma(bar, 0, err);
+  umma::fence_after_sync();
+  if (ok) {
+    float acc[CO];
+#pragma unroll
+    for (int c8 = 0; c8 < CO / 8; c8++) umma::ld8(tmem + ((uint32_t)(warp * 32) << 16) + c8 * 8, acc + c8 * 8);
+    const long long p = p0 + tid;
+    if (p < P) {
+      if (EPI == CONV_GELU) {
+        __nv_bfloat16* z = static_cast<__nv_bfloat16*>(out0) + p * CO;
+        __nv_bfloat16* a = static_cast<__nv_bfloat16*>(out1) + p * CO;
+#pragma unroll
+        for (int c8 = 0; c8 < CO / 8; c8++) {
+          __align__(16) __nv_bfloat16 zb[8], ab[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const float zz = acc[c8 * 8 + q] + bias[c8 * 8 + q];
+            zb[q] = __float2bfloat16_rn(zz);
+            ab[q] = __float2bfloat16_rn(gelu(zz));
+          }
+          *reinterpret_cast<uint4*>(z + c8 * 8) = *reinterpret_cast<const uint4*>(zb);
+          *reinterpret_cast<uint4*>(a + c8 * 8) = *reinterpret_cast<const uint4*>(ab);
+        }
+      } else if (EPI == CONV_LINEAR) {
+        float* o = static_cast<float*>(out0) + p * CO;
+#pragma unroll
+        for (int c4 = 0; c4 < CO / 4; c4++) {
+          float4 v;
+          v.x = acc[c4 * 4 + 0] + bias[c4 * 4 + 0];
+          v.y = acc[c4 * 4 + 1] + bias[c4 * 4 + 1];
+          v.z = acc[c4 * 4 + 2] + bias[c4 * 4 + 2];
+          v.w = acc[c4 * 4 + 3] + bias[c4 * 4 + 3];
+          *reinterpret_cast<float4*>(o + c4 * 4) = v;
+        }
+      } else {
+        const __nv_bfloat16* zp = zprev + p * CO;
+        __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + p * CO;
+#pragma unroll
+        for (int c8 = 0; c8 < CO / 8; c8++) {
+          const uint4 zv = *reinterpret_cast<const uint4*>(zp + c8 * 8);
+          const __nv_bfloat16* zs = reinterpret_cast<const __nv_bfloat16*>(&zv);
+          __align__(16) __nv_bfloat16 db[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) db[q] = __float2bfloat16_rn(acc[c8 * 8 + q] * gelu_grad(__bfloat162float(zs[q])));
+          *reinterpret_cast<uint4*>(d + c8 * 8) = *reinterpret_cast<const uint4*>(db);
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, kCols);
+  }
+}
+
+template <int CIN, int CO>
+struct WgradSmem {
+  static constexpr int M = 9 * CIN;
+  static constexpr int MT = (M + 127) / 128;           // M = 128 tiles
+  static constexpr int KC = 64;                        // pixels per chunk
+  static constexpr uint32_t kLboA = MT * 16u * 128u;   // K-group (8 pixels) stride of A
+  static constexpr uint32_t kBytesA = (KC / 8) * kLboA;
+  static constexpr uint32_t kLboB = (CO / 8) * 128u;
+  static constexpr uint32_t kBytesB = (KC / 8) * kLboB;
+  static constexpr uint32_t kOffBar = kBytesA + kBytesB;
+  static constexpr uint32_t kBytes = kOffBar + 16u;
+};
+
+// dW[co][t][ci] += sum_p dz[p][co] * x[p + tap t][ci] over this CTA's pixel
+// chunks; accumulator tile i (rows m = 128 i + lane, m = t * CIN + ci) sits
+// in tensor-memory columns [32 i, 32 i + CO).
+template <int CIN, int CO>
+__global__ void __launch_bounds__(128) wgrad_kernel(const __nv_bfloat16* __restrict__ x,
+                                                    const __nv_bfloat16* __restrict__ dz, int batch, int h, int w,
+                                                    float* __restrict__ dw, int* __restrict__ err) {
+  using S = WgradSmem<CIN, CO>;
+  constexpr uint32_t kCols = umma::tmem_cols(32 * S::MT);
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + S::kBytesA;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const long long P = (long long)batch * h * w;
+  const long long nchunks = (P + S::KC - 1) / S::KC;
+
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  // Rows M .. 128*MT-1 of A stay zero.
+  constexpr int kPadGroups = S::MT * 16 - S::M / 8;
+  for (int c = tid; c < (S::KC / 8) * kPadGroups * 8; c += 128) {
+    const int kg = c / (kPadGroups * 8), r = c - kg * kPadGroups * 8;
+    *reinterpret_cast<uint4*>(sA + kg * S::kLboA + (S::M / 8) * 128 + r * 16) = make_uint4(0u, 0u, 0u, 0u);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t idesc = umma::idesc_bf16(128, CO, true, true);
+  const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+  uint32_t phase = 0;
+  bool ok = true, any = false;
+  for (long long ch = blockIdx.x; ch < nchunks && ok; ch += gridDim.x) {
+    const long long p0 = ch * S::KC;
+    for (int c = tid; c < 9 * S::KC * (CIN / 8); c += 128) {
+      const int g = c % (CIN / 8);
+      const int j = (c / (CIN / 8)) % S::KC;
+      const int t = c / (S::KC * (CIN / 8));
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      const long long p = p0 + j;
+      if (p < P) {
+        const int x0 = (int)(p % w);
+        const long long r = p / w;
+        const int y0 = (int)(r % h);
+        const long long b = r / h;
+        const int yy = wrap(y0 + t / 3 - 1, h), xx = wrap(x0 + t % 3 - 1, w);
+        v = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CIN + g * 8);
+      }
+      *reinterpret_cast<uint4*>(sA + (t * (CIN / 8) + g) * 128 + (j % 8) * 16 + (j / 8) * S::kLboA) = v;
+    }
+    for (int c = tid; c < S::KC * (CO / 8); c += 128) {
+      const int g = c % (CO / 8), j = c / (CO / 8);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      const long long p = p0 + j;
+      if (p < P) v = *reinterpret_cast<const uint4*>(dz + p * CO + g * 8);
+      *reinterpret_cast<uint4*>(sB + g * 128 + (j % 8) * 16 + (j / 8) * S::kLboB) = v;
+    }
+    fence_proxy_async_smem();
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (tid == 0) {
+#pragma unroll
+      for (int kk = 0; kk < S::KC / 16; kk++)
+#pragma unroll
+        for (int i = 0; i < S::MT; i++) {
+          const uint64_t da = umma::desc(a0 + i * 2048 + kk * 2 * S::kLboA, S::kLboA, 128);
+          const uint64_t db = umma::desc(b0 + kk * 2 * S::kLboB, S::kLboB, 128);
+          umma::mma_bf16(tmem + 32 * i, da, db, idesc, (any || kk) ? 1u : 0u);
+        }
+      umma::commit(bar);
+    }
+    __syncwarp();
+    ok = wait_mma(bar, phase, err);
+    phase ^= 1u;
+    any = true;
+    umma::fence_after_sync();
+    ok = __syncthreads_and(ok);  // every warp agrees before the tiles are rewritten
+  }
+  if (any && ok) {
+#pragma unroll 1
+    for (int i = 0; i < S::MT; i++) {
+      float acc[CO];
+#pragma unroll
+      for (int c8 = 0; c8 < CO / 8; c8++)
+        umma::ld8(tmem + ((uint32_t)(warp * 32) << 16) + 32 * i + c8 * 8, acc + c8 * 8);
+      const int m = 128 * i + tid;
+      if (m < S::M)
+#pragma unroll
+        for (int co = 0; co < CO; co++) atomicAdd(dw + (size_t)co * S::M + m, acc[co]);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, kCols);
+  }
+}
+
+// db[co] += sum_p dz[p][co].
+template <int CO>
+__global__ void __launch_bounds__(256) bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, long long P,
+                                                        float* __restrict__ db) {
+  __shared__ float part[CO];
+  if (threadIdx.x < CO) part[threadIdx.x] = 0.f;
+  __syncthreads();
+  const int c = threadIdx.x % CO;
+  float s = 0.f;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P * CO; i += (long long)gridDim.x * blockDim.x)
+    s += __bfloat162float(dz[(i / CO) * CO + c]);
+  atomicAdd(&part[c], s);
+  __syncthreads();
+  if (threadIdx.x < CO) atomicAdd(db + threadIdx.x, part[threadIdx.x]);
+}
+
+template <class K>
+cudaError_t set_smem(K kernel, uint32_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int CG, int CO, int EPI>
+cudaError_t launch_conv(const __nv_bfloat16* x, int batch, int h, int w, const __nv_bfloat16* wt, const float* bias,
+                        const __nv_bfloat16* zprev, void* out0, void* out1, int* err, cudaStream_t s) {
+  using S = ConvSmem<CG, CO>;
+  auto k = conv3x3_kernel<CG, CO, EPI>;
+  static bool attr = false;  // per process; the attribute is per device and cheap to set again
+  if (!attr) {
+    const cudaError_t e = set_smem(k, S::kBytes);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const long long P = (long long)batch * h * w;
+  const unsigned grid = (unsigned)((P + 127) / 128);
+  k<<<grid, 128, S::kBytes, s>>>(x, wt, bias, zprev, batch, h, w, out0, out1, err);
+  return cudaGetLastError();
+}
+
+template <int CIN, int CO>
+cudaError_t launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, int batch, int h, int w, float* dw,
+                         float* db, int* err, cudaStream_t s) {
+  using S = WgradSmem<CIN, CO>;
+  auto k = wgrad_kernel<CIN, CO>;
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = set_smem(k, S::kBytes);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long P = (long long)batch * h * w;
+  const long long nchunks = (P + S::KC - 1) / S::KC;
+  // Up to 4 CTAs per SM fit both shared memory and the 512 tensor-memory
+  // columns; each CTA takes several chunks so the atomics stay few.
+  long long grid = nchunks < 2LL * sms ? nchunks : 2LL * sms;
+  if (grid < 1) grid = 1;
+  k<<<(unsigned)grid, 128, S::kBytes, s>>>(x, dz, batch, h, w, dw, err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !db) return e;
+  const long long tot = P * CO;
+  long long bg = (tot + 255) / 256;
+  if (bg > 4LL * sms) bg = 4LL * sms;
+  if (bg < 1) bg = 1;
+  bias_grad_kernel<CO><<<(unsigned)bg, 256, 0, s>>>(dz, P, db);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t conv3x3(int mode, const __nv_bfloat16* x, int batch, int h, int w, int c_in, const __nv_bfloat16* wt,
+                    const float* bias, int c_out, const __nv_bfloat16* zprev, void* out0, void* out1, int* err,
+                    cudaStream_t s) {
+  if (mode == CONV_GELU && c_in == 32 && c_out == 32)
+    return launch_conv<32, 32, CONV_GELU>(x, batch, h, w, wt, bias, zprev, out0, out1, err, s);
+  if (mode == CONV_LINEAR && c_in == 32 && c_out == 16)
+    return launch_conv<32, 16, CONV_LINEAR>(x, batch, h, w, wt, bias, zprev, out0, out1, err, s);
+  if (mode == CONV_DGELU && c_in == 16 && c_out == 32)
+    return launch_conv<16, 32, CONV_DGELU>(x, batch, h, w, wt, bias, zprev, out0, out1, err, s);
+  if (mode == CONV_DGELU && c_in == 32 && c_out == 32)
+    return launch_conv<32, 32, CONV_DGELU>(x, batch, h, w, wt, bias, zprev, out0, out1, err, s);
+  return cudaErrorNotSupported;
+}
+
+cudaError_t conv3x3_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, int batch, int h, int w, int c_in,
+                          int c_out, float* dw, float* db, int* err, cudaStream_t s) {
+  if (c_in == 32 && c_out == 32) return launch_wgrad<32, 32>(x, dz, batch, h, w, dw, db, err, s);
+  if (c_in == 32 && c_out == 16) return launch_wgrad<32, 16>(x, dz, batch, h, w, dw, db, err, s);
+  return cudaErrorNotSupported;
+}
+
+}  // namespace learned
+}  // namespace pmhd

@@ -29,6 +29,7 @@ ORDER_FIRST, ORDER_MUSCL = 0, 1
 SOLVER_HLL, SOLVER_HLLD = 0, 1
 PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D, PROBLEM_BRIO_WU_TORUS = 0, 1, 2, 3, 4
 LAYOUT_INTERIOR, LAYOUT_GHOSTED = 0, 1
+CONV_GELU, CONV_LINEAR, CONV_DGELU = 0, 1, 2
 
 PRECISIONS = {"fp64": FP64, "fp32": FP32, "mixed": MIXED}
 
@@ -40,6 +41,7 @@ EXPORTS = (
     "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state", "pmhd_advance_noalloc",
     "pmhd_ensemble_describe_default", "pmhd_ensemble_create", "pmhd_ensemble_advance",
     "pmhd_ensemble_member_stats", "pmhd_ensemble_get_state", "pmhd_ensemble_destroy",
+    "pmhd_conv3x3", "pmhd_conv3x3_wgrad",
 )
 
 
@@ -132,6 +134,8 @@ def load():
         "pmhd_ensemble_member_stats": ([vp, i, P(Stats)], i),
         "pmhd_ensemble_get_state": ([vp, i, vp, i], i),
         "pmhd_ensemble_destroy": ([vp], i),
+        "pmhd_conv3x3": ([i, vp, i, i, i, i, vp, P(ctypes.c_float), i, vp, vp, vp, vp], i),
+        "pmhd_conv3x3_wgrad": ([vp, vp, i, i, i, i, i, P(ctypes.c_float), P(ctypes.c_float), vp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

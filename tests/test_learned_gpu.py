@@ -1,0 +1,175 @@
+"""GPU checks of the BF16 tensor-core convolutions (pmhd_conv3x3,
+pmhd_conv3x3_wgrad) against the float64 network oracle.
+
+Two kinds of case per kernel: small-integer data, for which every product
+and partial sum is exact in the kernels' fp32 accumulators, so the results
+must equal the oracle's exactly (any operand-layout mistake shows as a wrong
+value, not a small error); and Gaussian data at sizes with partial tiles,
+within the tolerances of bf16 outputs (8 significant bits) and fp32
+accumulation.
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import cnn_oracle as C  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev_bf16(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).cuda()
+
+
+def _dev_f32(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def _host(t):
+    import torch
+    return t.float().cpu().numpy().astype(np.float64)
+
+
+def _conv(pmhd, mode, x, W, b, c_out, zprev=None):
+    import torch
+    B, H, Wd, cin = x.shape
+    xd, wd = _dev_bf16(x), _dev_bf16(W)
+    bd = _dev_f32(b) if b is not None else None
+    P = B * H * Wd
+    if mode == pmhd.CONV_GELU:
+        o0 = torch.empty((B, H, Wd, c_out), dtype=torch.bfloat16, device="cuda")
+        o1 = torch.empty_like(o0)
+    elif mode == pmhd.CONV_LINEAR:
+        o0 = torch.empty((B, H, Wd, c_out), dtype=torch.float32, device="cuda")
+        o1 = None
+    else:
+        o0 = torch.empty((B, H, Wd, c_out), dtype=torch.bfloat16, device="cuda")
+        o1 = None
+    zd = _dev_bf16(zprev) if zprev is not None else None
+    rc = pmhd.load().pmhd_conv3x3(mode, xd.data_ptr(), B, H, Wd, cin, wd.data_ptr(),
+                                  ctypes.cast(bd.data_ptr(), ctypes.POINTER(ctypes.c_float)) if bd is not None else None,
+                                  c_out, zd.data_ptr() if zd is not None else None, o0.data_ptr(),
+                                  o1.data_ptr() if o1 is not None else None, None)
+    assert rc == pmhd.OK, pmhd.strerror(rc)
+    return _host(o0), (_host(o1) if o1 is not None else None)
+
+
+def _wgrad(pmhd, x, dz):
+    import torch
+    B, H, Wd, cin = x.shape
+    co = dz.shape[3]
+    dw = torch.zeros((co, 9, cin), dtype=torch.float32, device="cuda")
+    db = torch.zeros((co,), dtype=torch.float32, device="cuda")
+    fp = ctypes.POINTER(ctypes.c_float)
+    rc = pmhd.load().pmhd_conv3x3_wgrad(_dev_bf16(x).data_ptr(), _dev_bf16(dz).data_ptr(), B, H, Wd, cin, co,
+                                        ctypes.cast(dw.data_ptr(), fp), ctypes.cast(db.data_ptr(), fp), None)
+    assert rc == pmhd.OK, pmhd.strerror(rc)
+    return _host(dw), _host(db)
+
+
+def _ints(rng, shape, p_nonzero=1.0):
+    v = rng.integers(-1, 2, size=shape).astype(np.float64)
+    if p_nonzero < 1.0:
+        v *= rng.random(shape) < p_nonzero
+    return v
+
+
+def _bf(a):
+    return C.bf16_round(a).astype(np.float64)
+
+
+SHAPES = [(1, 8, 16), (2, 9, 20), (1, 64, 64), (3, 17, 33)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_forward_gelu_exact_on_integers(pmhd_lib, shape):
+    rng = np.random.default_rng(10)
+    x = _ints(rng, shape + (32,))
+    W = _ints(rng, (32, 9, 32), 0.2)
+    b = rng.integers(-3, 4, 32).astype(np.float64)
+    z, a = _conv(pmhd_lib, pmhd_lib.CONV_GELU, x, W, b, 32)
+    zr = C.conv3x3(x, W, b)
+    np.testing.assert_array_equal(z, zr)
+    # gelu is evaluated in fp32 on the device: allow one bf16 ulp.
+    np.testing.assert_allclose(a, _bf(C.gelu(zr)), rtol=2.0 ** -7, atol=1e-30)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_forward_linear_exact_on_integers(pmhd_lib, shape):
+    rng = np.random.default_rng(11)
+    x = _ints(rng, shape + (32,))
+    W = _ints(rng, (16, 9, 32))
+    b = rng.integers(-3, 4, 16).astype(np.float64)
+    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_LINEAR, x, W, b, 16)
+    np.testing.assert_array_equal(out, C.conv3x3(x, W, b))
+
+
+@pytest.mark.parametrize("cin", [16, 32])
+@pytest.mark.parametrize("shape", SHAPES[:3])
+def test_backward_input_exact_on_integers(pmhd_lib, shape, cin):
+    """x = the layer's output gradient (cin channels), W the layer weight
+    [cin][9][32]; the kernel takes W transposed to [32][9][cin]."""
+    rng = np.random.default_rng(12)
+    dz = _ints(rng, shape + (cin,))
+    W = _ints(rng, (cin, 9, 32), 0.3)
+    zprev = _bf(rng.normal(0, 1.0, shape + (32,)))
+    Wt = np.ascontiguousarray(W.transpose(2, 1, 0))
+    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz, Wt, None, 32, zprev=zprev)
+    da = C.conv3x3_backward_input(dz, W)  # exact integers
+    ref = C.bf16_round((da * C.gelu_grad(zprev)).astype(np.float32)).astype(np.float64)
+    # gelu' is evaluated in fp32 on the device: allow one bf16 ulp.
+    np.testing.assert_allclose(out, ref, rtol=2.0 ** -7, atol=0)
+    np.testing.assert_array_equal(out == 0, ref == 0)
+
+
+@pytest.mark.parametrize("cout", [32, 16])
+@pytest.mark.parametrize("shape", SHAPES)
+def test_weight_gradient_exact_on_integers(pmhd_lib, shape, cout):
+    rng = np.random.default_rng(13)
+    x = _ints(rng, shape + (32,))
+    dz = _ints(rng, shape + (cout,))
+    dw, db = _wgrad(pmhd_lib, x, dz)
+    dwr, dbr = C.conv3x3_backward_weight(x, dz)
+    np.testing.assert_array_equal(dw, dwr)
+    np.testing.assert_array_equal(db, dbr)
+
+
+def test_gaussian_layers_within_bf16_tolerance(pmhd_lib):
+    rng = np.random.default_rng(14)
+    shape = (2, 33, 47)
+    x = _bf(rng.normal(0, 1, shape + (32,)))
+    W1 = _bf(rng.normal(0, 0.08, (32, 9, 32)))
+    b1 = rng.normal(0, 0.1, 32).astype(np.float32).astype(np.float64)
+    z, a = _conv(pmhd_lib, pmhd_lib.CONV_GELU, x, W1, b1, 32)
+    zr = C.conv3x3(x, W1, b1)
+    scale = np.abs(zr).max()
+    np.testing.assert_allclose(z, zr, rtol=2.0 ** -8, atol=1e-5 * scale)
+    np.testing.assert_allclose(a, C.gelu(zr), rtol=2.0 ** -7, atol=1e-5 * scale)
+    W3 = _bf(rng.normal(0, 0.08, (16, 9, 32)))
+    b3 = rng.normal(0, 0.1, 16).astype(np.float32).astype(np.float64)
+    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_LINEAR, a, W3, b3, 16)
+    outr = C.conv3x3(a, W3, b3)
+    np.testing.assert_allclose(out, outr, rtol=1e-5, atol=1e-5 * np.abs(outr).max())
+    dz = _bf(rng.normal(0, 1e-3, shape + (16,)))
+    dw, db = _wgrad(pmhd_lib, a, dz)
+    dwr, dbr = C.conv3x3_backward_weight(a, dz)
+    np.testing.assert_allclose(dw, dwr, rtol=1e-4, atol=1e-4 * np.abs(dwr).max())
+    np.testing.assert_allclose(db, dbr, rtol=1e-4, atol=1e-4 * np.abs(dbr).max())
+
+
+def test_unsupported_channel_counts_are_rejected(pmhd_lib):
+    import torch
+    x = torch.zeros((1, 8, 8, 24), dtype=torch.bfloat16, device="cuda")
+    w = torch.zeros((24, 9, 24), dtype=torch.bfloat16, device="cuda")
+    b = torch.zeros((24,), dtype=torch.float32, device="cuda")
+    o = torch.zeros((1, 8, 8, 24), dtype=torch.bfloat16, device="cuda")
+    rc = pmhd_lib.load().pmhd_conv3x3(pmhd_lib.CONV_GELU, x.data_ptr(), 1, 8, 8, 24, w.data_ptr(),
+                                      ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_float)), 24, None,
+                                      o.data_ptr(), o.data_ptr(), None)
+    assert rc == pmhd_lib.ERR_UNSUPPORTED

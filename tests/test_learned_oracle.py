@@ -1,0 +1,64 @@
+"""CPU checks of the network oracle (oracle/cnn_oracle.py): its analytic
+gradients against central finite differences in float64, the transposed
+convolution against the adjoint identity, and its bfloat16 rounding."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import cnn_oracle as C  # noqa: E402
+
+
+def _params(rng, widths):
+    return [(rng.normal(0, 0.4, (co, 9, ci)), rng.normal(0, 0.1, co)) for ci, co in zip(widths[:-1], widths[1:])]
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    vals = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -2.5, 1e-3, 3.0e38], dtype=np.float32)
+    bits = C.to_bf16_bits(vals)
+    assert list(bits[:4]) == [0x3F80, 0x3F80, 0x3F82, 0xC020]
+    back = C.from_bf16_bits(bits)
+    assert np.all(np.abs(back - vals) <= np.abs(vals) * 2.0 ** -8)
+
+
+def test_adjoint_of_the_convolution():
+    rng = np.random.default_rng(1)
+    x = rng.normal(size=(2, 5, 7, 3))
+    dz = rng.normal(size=(2, 5, 7, 4))
+    W = rng.normal(size=(4, 9, 3))
+    lhs = np.sum(dz * C.conv3x3(x, W))
+    rhs = np.sum(x * C.conv3x3_backward_input(dz, W))
+    assert abs(lhs - rhs) < 1e-10 * abs(lhs)
+
+
+def test_network_gradients_match_finite_differences():
+    rng = np.random.default_rng(2)
+    widths = [3, 4, 4, 2]
+    params = _params(rng, widths)
+    x = rng.normal(size=(1, 4, 5, 3))
+    target = rng.normal(size=(1, 4, 5, 2))
+    loss, grads = C.net_loss_and_grads(x, params, target, 2)
+    h = 1e-6
+    for li, (W, b) in enumerate(params):
+        for idx in [(0, 0, 0), (1, 4, 2), (W.shape[0] - 1, 8, W.shape[2] - 1)]:
+            Wp = [(w.copy(), bb.copy()) for w, bb in params]
+            Wm = [(w.copy(), bb.copy()) for w, bb in params]
+            Wp[li][0][idx] += h
+            Wm[li][0][idx] -= h
+            fd = (C.net_loss_and_grads(x, Wp, target, 2)[0] - C.net_loss_and_grads(x, Wm, target, 2)[0]) / (2 * h)
+            assert abs(fd - grads[li][0][idx]) < 1e-6 * max(1.0, abs(fd)), (li, idx)
+        Wp = [(w.copy(), bb.copy()) for w, bb in params]
+        Wm = [(w.copy(), bb.copy()) for w, bb in params]
+        Wp[li][1][0] += h
+        Wm[li][1][0] -= h
+        fd = (C.net_loss_and_grads(x, Wp, target, 2)[0] - C.net_loss_and_grads(x, Wm, target, 2)[0]) / (2 * h)
+        assert abs(fd - grads[li][1][0]) < 1e-6 * max(1.0, abs(fd)), (li, "bias")
+
+
+def test_gelu_derivative_matches_finite_differences():
+    z = np.linspace(-5, 5, 41)
+    h = 1e-6
+    fd = (C.gelu(z + h) - C.gelu(z - h)) / (2 * h)
+    np.testing.assert_allclose(C.gelu_grad(z), fd, atol=1e-8)
