@@ -256,6 +256,78 @@ int pmhd_conv3x3(int mode, const void* x, int batch, int h, int w, int c_in, con
 int pmhd_conv3x3_wgrad(const void* x, const void* dz, int batch, int h, int w, int c_in, int c_out, float* dweight,
                        float* dbias, void* stream);
 
+/* ---- Learned coarse-grid correction -------------------------------------------
+ * No counterpart in the reference.  A periodic problem runs on a coarse grid
+ * (nx x ny) with the plain solver; after every step a small network (three
+ * 3x3 convolutions, 32 channels, GELU; BF16 tensor-core kernels with fp32
+ * accumulation) predicts the difference between the fine solution (refine x
+ * finer, restricted by block averages) and the coarse step, from the coarse
+ * state and its step increment.  The correction is applied only when the
+ * corrected state keeps positive density and pressure and its ||div B||_1
+ * grows by at most div_tol relative to the uncorrected step; otherwise the
+ * plain coarse step stands (counted as a rejection).  Training pairs come
+ * from the solver itself (pmhd_learned_generate: fine and coarse runs of a
+ * problem); training runs on the device with the project's own forward and
+ * backward kernels and Adam.  All four boundaries are periodic; states are
+ * fp64 (precision PMHD_FP64 or PMHD_MIXED for both solvers). */
+typedef struct pmhd_learned pmhd_learned;
+
+typedef struct {
+  int nx, ny;                 /* coarse grid (even sizes)                        */
+  int refine;                 /* fine / coarse ratio of the training pairs (4)   */
+  double x_min, x_max, y_min, y_max;
+  double gamma, cfl, alpha;
+  int precision;              /* PMHD_FP64 or PMHD_MIXED                         */
+  int device;
+  int max_pairs;              /* capacity of the pair store (512)                */
+  unsigned long long seed;    /* weight initialisation and minibatch order       */
+  double div_tol;             /* allowed relative growth of ||div B||_1 (0.5)    */
+} pmhd_learned_config;
+
+typedef struct {
+  long long steps;            /* coarse (or fine) steps taken                    */
+  double t;
+  long long accepted;         /* corrections applied                             */
+  long long rejected_positivity, rejected_divergence;
+  double device_ms;           /* device time of the time loop                    */
+  double wall_ms;             /* wall-clock time of the time loop                */
+  int status;
+} pmhd_learned_stats;
+
+int pmhd_learned_config_default(pmhd_learned_config* cfg);
+int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out);
+int pmhd_learned_destroy(pmhd_learned* L);
+
+/* Runs `problem` (params as for pmhd_init_problem) on the fine grid to
+ * t_end; before every coarse step it restricts the fine state, takes one
+ * plain coarse step from it, advances the fine run to the same time and
+ * stores (before, coarse step, restricted fine) as a pair every `every`
+ * steps, until the store is full.  *added (may be NULL) = pairs stored. */
+int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
+                          int* added);
+int pmhd_learned_num_pairs(const pmhd_learned* L);
+
+/* `iters` Adam steps (cosine decay from lr) on minibatches of `batch` pairs
+ * drawn uniformly; losses (may be NULL, `iters` floats) receives the
+ * minibatch mean squared error of the normalised correction per step.  The
+ * input/output normalisation is fixed from the pairs at the first call. */
+int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* losses);
+
+/* Coarse run of `problem` from the restricted fine initial state to t_end,
+ * corrected (use_net = 1) or plain (0); host_out (may be NULL) receives the
+ * final coarse interior state, [ny][nx][9] doubles. */
+int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int use_net,
+                     double* host_out, pmhd_learned_stats* stats);
+
+/* Fine run at `refine` x the coarse resolution, restricted onto the coarse
+ * grid at t_end (the judge of the coarse runs); host_out as above. */
+int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int refine,
+                          double* host_out, pmhd_learned_stats* stats);
+
+/* Network weights and normalisation to / from a file. */
+int pmhd_learned_save(const pmhd_learned* L, const char* path);
+int pmhd_learned_load(pmhd_learned* L, const char* path);
+
 /* ---- Allocation-free time loop ----------------------------------------------
  * No counterpart in the reference: its program always cudaMallocs five state
  * arrays.  For callers that must not allocate device memory while they run

@@ -12,12 +12,12 @@ finite differences in float64 (tests/test_learned_oracle.py).
 Conventions (the kernels' own): images are NHWC arrays [batch, h, w, c],
 periodic in y and x; weights W[c_out, 9, c_in] with tap t = (dy+1)*3 +
 (dx+1) and out(y, x) = sum_t W[:, t, :] @ x(y+dy, x+dx) + b; GELU is the
-erf form 0.5 z (1 + erf(z / sqrt 2)).
+erf form 0.5 z (1 + erf(z / sqrt 2)) = 0.5 z erfc(-z / sqrt 2).
 """
 import math
 
 import numpy as np
-from scipy.special import erf
+from scipy.special import erfc
 
 TAPS = [(t // 3 - 1, t % 3 - 1) for t in range(9)]
 
@@ -40,11 +40,12 @@ def from_bf16_bits(u):
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / math.sqrt(2.0)))
+    # 1 + erf(u) = erfc(-u): no cancellation in the left tail.
+    return 0.5 * z * erfc(-z / math.sqrt(2.0))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    return 0.5 * erfc(-z / math.sqrt(2.0)) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
 
 
 def shift(x, dy, dx):

@@ -11,7 +11,16 @@ namespace {
 
 __device__ int g_conv_err;  // set by a kernel whose bounded wait expired
 
+// Device address of the error word; the first call on a device also sets the
+// kernels' shared-memory limits there.
 int* error_word() {
+  static int prepared_dev = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  if (dev != prepared_dev) {
+    if (pmhd::learned::conv_prepare() != cudaSuccess) return nullptr;
+    prepared_dev = dev;
+  }
   int* p = nullptr;
   if (cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_conv_err) != cudaSuccess) return nullptr;
   return p;

@@ -12,9 +12,9 @@
 // wrap) into K-major shared-memory tiles, one thread issues 9 * c_in / 16
 // tcgen05.mma, the four warps read the 128 x N accumulator back with
 // tcgen05.ld and run the epilogue.  Weight gradient: D[(t, c_in)][c_out] =
-// sum over pixels of x(p + tap) dz(p)^T, K = pixels, both operands gathered
-// MN-major (channel vectors are contiguous in NHWC), three M = 128 tiles
-// accumulated over 64-pixel chunks, summed over CTAs with fp32 atomics.
+// sum over pixels of x(p + tap) dz(p)^T, K = pixels: blocks of 8 pixels x 8
+// channels are transposed in registers into K-major tiles, three M = 128
+// tiles accumulate over 64-pixel chunks, CTAs sum with fp32 atomics.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -28,12 +28,31 @@ namespace {
 
 constexpr uint32_t kWaitPolls = 1u << 22;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in the erf form, written with erfc (1 + erf(u) = erfc(-u)) so the
+// left tail keeps its relative accuracy instead of cancelling to zero.
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * erfcf(-z * 0.70710678118654752f); }
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  return 0.5f * erfcf(-z * 0.70710678118654752f) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+__device__ __forceinline__ uint32_t word_of(const uint4& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+// Row `ch` of the 8 x 8 bf16 transpose of v[0..7] (v[q] = 8 channels of
+// pixel q): the 8 pixels' values of channel ch, pixel q in halfword q.
+__device__ __forceinline__ uint4 transpose_row(const uint4 (&v)[8], int ch) {
+  const uint32_t sel = (ch & 1) ? 0x7632u : 0x5410u;
+  const int wi = ch >> 1;
+  uint4 r;
+  r.x = __byte_perm(word_of(v[0], wi), word_of(v[1], wi), sel);
+  r.y = __byte_perm(word_of(v[2], wi), word_of(v[3], wi), sel);
+  r.z = __byte_perm(word_of(v[4], wi), word_of(v[5], wi), sel);
+  r.w = __byte_perm(word_of(v[6], wi), word_of(v[7], wi), sel);
+  return r;
+}
 
 // Bounded wait for the MMA batch; on expiry record the error and wait once
 // more (bounded) so tensor memory is not released under a running MMA.
@@ -242,34 +261,50 @@ __global__ void __launch_bounds__(128) wgrad_kernel(const __nv_bfloat16* __restr
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
-  constexpr uint32_t idesc = umma::idesc_bf16(128, CO, true, true);
+  constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
   const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
   uint32_t phase = 0;
   bool ok = true, any = false;
   for (long long ch = blockIdx.x; ch < nchunks && ok; ch += gridDim.x) {
     const long long p0 = ch * S::KC;
-    for (int c = tid; c < 9 * S::KC * (CIN / 8); c += 128) {
+    // A: blocks of 8 pixels x 8 channels, transposed in registers so that
+    // each row (one tap and channel) holds 8 consecutive pixels (K-major).
+    for (int c = tid; c < 9 * (S::KC / 8) * (CIN / 8); c += 128) {
       const int g = c % (CIN / 8);
-      const int j = (c / (CIN / 8)) % S::KC;
-      const int t = c / (S::KC * (CIN / 8));
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      const long long p = p0 + j;
-      if (p < P) {
-        const int x0 = (int)(p % w);
-        const long long r = p / w;
-        const int y0 = (int)(r % h);
-        const long long b = r / h;
-        const int yy = wrap(y0 + t / 3 - 1, h), xx = wrap(x0 + t % 3 - 1, w);
-        v = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CIN + g * 8);
+      const int kg = (c / (CIN / 8)) % (S::KC / 8);
+      const int t = c / ((S::KC / 8) * (CIN / 8));
+      uint4 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        v[q] = make_uint4(0u, 0u, 0u, 0u);
+        const long long p = p0 + kg * 8 + q;
+        if (p < P) {
+          const int x0 = (int)(p % w);
+          const long long r = p / w;
+          const int y0 = (int)(r % h);
+          const long long b = r / h;
+          const int yy = wrap(y0 + t / 3 - 1, h), xx = wrap(x0 + t % 3 - 1, w);
+          v[q] = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CIN + g * 8);
+        }
       }
-      *reinterpret_cast<uint4*>(sA + (t * (CIN / 8) + g) * 128 + (j % 8) * 16 + (j / 8) * S::kLboA) = v;
+#pragma unroll
+      for (int ch = 0; ch < 8; ch++) {
+        const int m = t * CIN + g * 8 + ch;
+        *reinterpret_cast<uint4*>(sA + (m / 8) * 128 + (m % 8) * 16 + kg * S::kLboA) = transpose_row(v, ch);
+      }
     }
-    for (int c = tid; c < S::KC * (CO / 8); c += 128) {
-      const int g = c % (CO / 8), j = c / (CO / 8);
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      const long long p = p0 + j;
-      if (p < P) v = *reinterpret_cast<const uint4*>(dz + p * CO + g * 8);
-      *reinterpret_cast<uint4*>(sB + g * 128 + (j % 8) * 16 + (j / 8) * S::kLboB) = v;
+    // B: the output gradient, the same way (rows = output channels).
+    for (int c = tid; c < (S::KC / 8) * (CO / 8); c += 128) {
+      const int g = c % (CO / 8), kg = c / (CO / 8);
+      uint4 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const long long p = p0 + kg * 8 + q;
+        v[q] = p < P ? *reinterpret_cast<const uint4*>(dz + p * CO + g * 8) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int ch = 0; ch < 8; ch++)
+        *reinterpret_cast<uint4*>(sB + g * 128 + ch * 16 + kg * S::kLboB) = transpose_row(v, ch);
     }
     fence_proxy_async_smem();
     umma::fence_before_sync();
@@ -335,17 +370,13 @@ cudaError_t set_smem(K kernel, uint32_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+int g_sms = 0;  // SM count of the device the kernels were prepared on
+
 template <int CG, int CO, int EPI>
 cudaError_t launch_conv(const __nv_bfloat16* x, int batch, int h, int w, const __nv_bfloat16* wt, const float* bias,
                         const __nv_bfloat16* zprev, void* out0, void* out1, int* err, cudaStream_t s) {
   using S = ConvSmem<CG, CO>;
   auto k = conv3x3_kernel<CG, CO, EPI>;
-  static bool attr = false;  // per process; the attribute is per device and cheap to set again
-  if (!attr) {
-    const cudaError_t e = set_smem(k, S::kBytes);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
   const long long P = (long long)batch * h * w;
   const unsigned grid = (unsigned)((P + 127) / 128);
   k<<<grid, 128, S::kBytes, s>>>(x, wt, bias, zprev, batch, h, w, out0, out1, err);
@@ -357,15 +388,7 @@ cudaError_t launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, int ba
                          float* db, int* err, cudaStream_t s) {
   using S = WgradSmem<CIN, CO>;
   auto k = wgrad_kernel<CIN, CO>;
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = set_smem(k, S::kBytes);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = g_sms > 0 ? g_sms : 148;
   const long long P = (long long)batch * h * w;
   const long long nchunks = (P + S::KC - 1) / S::KC;
   // Up to 4 CTAs per SM fit both shared memory and the 512 tensor-memory
@@ -384,6 +407,19 @@ cudaError_t launch_wgrad(const __nv_bfloat16* x, const __nv_bfloat16* dz, int ba
 }
 
 }  // namespace
+
+cudaError_t conv_prepare() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 32, CONV_GELU>, ConvSmem<32, 32>::kBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 16, CONV_LINEAR>, ConvSmem<32, 16>::kBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_kernel<16, 32, CONV_DGELU>, ConvSmem<16, 32>::kBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 32, CONV_DGELU>, ConvSmem<32, 32>::kBytes);
+  if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 32>, WgradSmem<32, 32>::kBytes);
+  if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 16>, WgradSmem<32, 16>::kBytes);
+  return e;
+}
 
 cudaError_t conv3x3(int mode, const __nv_bfloat16* x, int batch, int h, int w, int c_in, const __nv_bfloat16* wt,
                     const float* bias, int c_out, const __nv_bfloat16* zprev, void* out0, void* out1, int* err,

@@ -11,6 +11,10 @@ namespace learned {
 enum ConvMode : int { CONV_GELU = 0, CONV_LINEAR = 1, CONV_DGELU = 2 };
 enum : int { PMHD_LEARNED_ERR_TIMEOUT = 1 };
 
+// Sets the kernels' shared-memory limits on the current device; call once
+// per device before the first launch (and before any stream capture).
+cudaError_t conv_prepare();
+
 // One 3x3 periodic convolution over NHWC bf16 images (see conv.cu).
 //   CONV_GELU:   out0 = z = conv(x) + bias (bf16), out1 = gelu(z) (bf16)
 //   CONV_LINEAR: out0 = conv(x) + bias (fp32)

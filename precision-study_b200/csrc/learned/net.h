@@ -1,0 +1,106 @@
+// net.h -- the learned coarse-grid correction's non-convolution kernels
+// (net.cu): features and targets from solver states, loss, Adam, restriction
+// of fine states, and the checked application of a correction.
+#ifndef PMHD_LEARNED_NET_H
+#define PMHD_LEARNED_NET_H
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pmhd {
+namespace learned {
+
+constexpr int kNVar = 9;
+constexpr int kFeat = 32;   // input channels (18 used: state and step increment)
+constexpr int kWidth = 32;  // hidden channels
+constexpr int kOut = 16;    // output channels (9 used: the correction)
+
+// fp64 state of `batch` grids: variable k of interior cell (i, j) of grid b at
+// u[offset + b*bstride + k*vstride + j*jstride + i*istride].
+struct StateView {
+  const double* u;
+  long long offset, bstride, vstride, jstride, istride;
+};
+
+inline StateView soa_view(const void* u, int pitch, long long plane) {
+  return StateView{static_cast<const double*>(u), 2LL * pitch + 2, 0, plane, pitch, 1};
+}
+inline StateView aos_view(const void* u, int nx, int ny) {
+  return StateView{static_cast<const double*>(u), 0, (long long)nx * ny * kNVar, 1, (long long)nx * kNVar, kNVar};
+}
+
+// Normalisation of the network's inputs and outputs.
+struct Norm {
+  float mu[2 * kNVar], inv_sig[2 * kNVar];  // features: state, step increment
+  float sig_out[kNVar], inv_out[kNVar];     // correction scale per variable (0 / 0: not corrected)
+};
+
+// Three 3x3 layers: 32 -> 32 (GELU) -> 32 (GELU) -> 16 (linear).
+struct NetLayout {
+  int w_off[3], b_off[3];  // offsets into the fp32 parameter vector
+  int cin[3], cout[3];
+  int n_params;
+};
+NetLayout net_layout();
+
+// Device pointers of one set of network weights.
+struct NetWeights {
+  float* theta;                  // fp32 parameters (weights then bias per layer)
+  __nv_bfloat16* wf[3];          // bf16 [cout][9][cin] (forward)
+  __nv_bfloat16* wb[3];          // bf16 [cin][9][cout] (backward to the input)
+};
+
+// Per-step work of a corrected run.
+struct CorrState {
+  double* before;      // SoA copy of the state before the step (solver layout)
+  double* cand;        // AoS interior candidate state
+  __nv_bfloat16* x;    // features [ny][nx][32]
+  __nv_bfloat16* z1, *a1, *z2, *a2;
+  float* out;          // network output [ny][nx][16]
+  // flags[0]: candidate not positive; sums[0..1]: ||divB||_1 after the step
+  // and of the candidate; counters[0..2]: accepted, rejected (positivity),
+  // rejected (divergence); accept: this step's decision.
+  int* flags;
+  double* sums;
+  unsigned long long* counters;
+  int* accept;
+  const Norm* norm;    // device copy
+};
+
+cudaError_t features(const StateView& after, const StateView& before, int batch, int nx, int ny, const Norm* norm,
+                     __nv_bfloat16* x, cudaStream_t s);
+cudaError_t targets(const StateView& after, const StateView& fine, int batch, int nx, int ny, const Norm* norm,
+                    float* tgt, cudaStream_t s);
+// sums[0..26] += per-variable sums of (after, after - before, fine - after),
+// sums[27..53] += their squares.
+cudaError_t moments(const StateView& before, const StateView& after, const StateView& fine, int batch, int nx,
+                    int ny, double* sums, cudaStream_t s);
+cudaError_t loss_grad(const float* out, const float* tgt, long long P, __nv_bfloat16* dz, float* loss_hist,
+                      const int* it, cudaStream_t s);
+cudaError_t adam(const NetLayout& L, NetWeights w, float* grad, float* m, float* v, const int* it, int iters,
+                 float lr, cudaStream_t s);
+cudaError_t weights_to_bf16(const NetLayout& L, NetWeights w, cudaStream_t s);
+cudaError_t gather_pairs(const int* schedule, const int* it, int batch, const __nv_bfloat16* feat_all,
+                         const float* tgt_all, long long pix_per_pair, __nv_bfloat16* feat, float* tgt,
+                         cudaStream_t s);
+cudaError_t increment(int* it, cudaStream_t s);
+// Block average of a fine SoA state (factor r) into a coarse AoS interior.
+cudaError_t restrict_state(const void* fine_u, int fpitch, long long fplane, int fnx, int fny, int r, double* coarse,
+                           cudaStream_t s);
+// AoS interior -> solver SoA with periodic ghost cells.
+cudaError_t load_periodic(const double* aos, void* u, int pitch, long long plane, int nx, int ny, cudaStream_t s);
+// Solver SoA interior -> AoS interior.
+cudaError_t store_interior(const void* u, int pitch, long long plane, int nx, int ny, double* aos, cudaStream_t s);
+
+// The correction of one step at parity p: candidate, checks, decision,
+// commit (see net.cu); ctrl tells whether the step was taken.
+cudaError_t correct_step(const CorrState& cs, void* u, int pitch, long long plane, int nx, int ny, double dx,
+                         double dy, double gamma, double div_tol, const Ctrl* ctrl, Ctrl* ctrl_w, int p,
+                         cudaStream_t s);
+
+}  // namespace learned
+}  // namespace pmhd
+
+#endif  // PMHD_LEARNED_NET_H

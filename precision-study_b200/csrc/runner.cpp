@@ -7,10 +7,16 @@ cudaError_t Runner::enqueue_steps(int nsteps) const {
   const Batch& b = batch[choice.ty_idx];
   for (int n = 0; n < nsteps; n++) {
     const int p = n & 1;
-    cudaError_t e = kt->stage(precision, hlld, 1, choice.ty_idx, b, single, p, choice.grid, stream);
+    cudaError_t e = pre_step ? pre_step(p) : cudaSuccess;
+    if (e != cudaSuccess) return e;
+    e = kt->stage(precision, hlld, 1, choice.ty_idx, b, single, p, choice.grid, stream);
     if (e != cudaSuccess) return e;
     e = kt->stage(precision, hlld, 2, choice.ty_idx, b, single, p, choice.grid, stream);
     if (e != cudaSuccess) return e;
+    if (post_step) {
+      e = post_step(p);
+      if (e != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
 }

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <vector>
 
 #include "kernel_api.h"
@@ -34,6 +35,9 @@ class Runner {
   Batch batch[kNumTileHeights];
   const Member* single = nullptr;  // host copy of a one-grid batch's member, or nullptr
   LaunchChoice choice;
+  // Optional work enqueued before and after every step (argument: the
+  // step's parity), captured into the graphs with the stage launches.
+  std::function<cudaError_t(int)> pre_step, post_step;
 
   // Enqueues `nsteps` steps (two stage launches each, parity 0, 1, 0, ...).
   cudaError_t enqueue_steps(int nsteps) const;

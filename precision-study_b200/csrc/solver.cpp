@@ -26,6 +26,7 @@
 #include "pmhd.h"
 #include "problems.h"
 #include "runner.h"
+#include "solver_internal.h"
 
 using namespace pmhd;
 
@@ -59,6 +60,37 @@ struct pmhd_solver {
   pmhd_stats stats;
   bool failed = false;
 };
+
+namespace pmhd {
+
+bool solver_view(pmhd_solver* s, SolverView* v) {
+  if (!s || !v) return false;
+  v->u = s->dU;
+  v->u1 = s->dU1;
+  v->pitch = s->pitch;
+  v->plane = s->plane;
+  v->nx = s->cfg.nx;
+  v->ny = s->cfg.ny;
+  v->dx = (s->cfg.x_max - s->cfg.x_min) / s->cfg.nx;
+  v->dy = (s->cfg.y_max - s->cfg.y_min) / s->cfg.ny;
+  v->gamma = s->cfg.gamma;
+  v->precision = s->cfg.precision;
+  v->stream = s->stream;
+  v->ctrl = s->dCtrl;
+  v->kt = s->kt;
+  return true;
+}
+
+void solver_set_step_hooks(pmhd_solver* s, std::function<cudaError_t(int)> pre,
+                           std::function<cudaError_t(int)> post) {
+  if (!s) return;
+  cudaStreamSynchronize(s->stream);
+  s->run.release();
+  s->run.pre_step = std::move(pre);
+  s->run.post_step = std::move(post);
+}
+
+}  // namespace pmhd
 
 namespace {
 

@@ -42,6 +42,9 @@ EXPORTS = (
     "pmhd_ensemble_describe_default", "pmhd_ensemble_create", "pmhd_ensemble_advance",
     "pmhd_ensemble_member_stats", "pmhd_ensemble_get_state", "pmhd_ensemble_destroy",
     "pmhd_conv3x3", "pmhd_conv3x3_wgrad",
+    "pmhd_learned_config_default", "pmhd_learned_create", "pmhd_learned_destroy", "pmhd_learned_generate",
+    "pmhd_learned_num_pairs", "pmhd_learned_train", "pmhd_learned_run", "pmhd_learned_fine_run",
+    "pmhd_learned_save", "pmhd_learned_load",
 )
 
 
@@ -99,6 +102,30 @@ class MemberDesc(ctypes.Structure):
         return d
 
 
+class LearnedConfig(ctypes.Structure):
+    """pmhd_learned_config."""
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("refine", ctypes.c_int),
+        ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+        ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("alpha", ctypes.c_double),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int), ("max_pairs", ctypes.c_int),
+        ("seed", ctypes.c_ulonglong), ("div_tol", ctypes.c_double),
+    ]
+
+
+class LearnedStats(ctypes.Structure):
+    """pmhd_learned_stats."""
+    _fields_ = [
+        ("steps", ctypes.c_longlong), ("t", ctypes.c_double), ("accepted", ctypes.c_longlong),
+        ("rejected_positivity", ctypes.c_longlong), ("rejected_divergence", ctypes.c_longlong),
+        ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double), ("status", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -136,6 +163,16 @@ def load():
         "pmhd_ensemble_destroy": ([vp], i),
         "pmhd_conv3x3": ([i, vp, i, i, i, i, vp, P(ctypes.c_float), i, vp, vp, vp, vp], i),
         "pmhd_conv3x3_wgrad": ([vp, vp, i, i, i, i, i, P(ctypes.c_float), P(ctypes.c_float), vp], i),
+        "pmhd_learned_config_default": ([P(LearnedConfig)], i),
+        "pmhd_learned_create": ([P(LearnedConfig), P(vp)], i),
+        "pmhd_learned_destroy": ([vp], i),
+        "pmhd_learned_generate": ([vp, i, P(d), i, d, i, P(i)], i),
+        "pmhd_learned_num_pairs": ([vp], i),
+        "pmhd_learned_train": ([vp, i, i, d, P(ctypes.c_float)], i),
+        "pmhd_learned_run": ([vp, i, P(d), i, d, i, P(d), P(LearnedStats)], i),
+        "pmhd_learned_fine_run": ([vp, i, P(d), i, d, i, P(d), P(LearnedStats)], i),
+        "pmhd_learned_save": ([vp, ctypes.c_char_p], i),
+        "pmhd_learned_load": ([vp, ctypes.c_char_p], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -362,6 +399,91 @@ class Ensemble:
         out = np.empty(shape, dtype=self.dtype)
         _check(load().pmhd_ensemble_get_state(self._h, k, out.ctypes.data, layout), "pmhd_ensemble_get_state")
         return out
+
+
+def _params_arg(params):
+    if params is None or len(params) == 0:
+        return None, 0
+    return (ctypes.c_double * len(params))(*params), len(params)
+
+
+class Learned:
+    """Learned coarse-grid correction (a pmhd_learned handle): training pairs
+    from the solver, device training, corrected and plain coarse runs, and
+    the fine run that judges them."""
+
+    def __init__(self, **kw):
+        L = load()
+        c = LearnedConfig()
+        _check(L.pmhd_learned_config_default(ctypes.byref(c)), "pmhd_learned_config_default")
+        for k, val in kw.items():
+            if k == "precision" and isinstance(val, str):
+                val = PRECISIONS[val]
+            if k == "domain":
+                c.x_min, c.x_max, c.y_min, c.y_max = val
+                continue
+            setattr(c, k, val)
+        self.cfg = c
+        h = ctypes.c_void_p()
+        _check(L.pmhd_learned_create(ctypes.byref(c), ctypes.byref(h)), "pmhd_learned_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pmhd_learned_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_pairs(self):
+        return load().pmhd_learned_num_pairs(self._h)
+
+    def generate(self, problem=PROBLEM_ORSZAG_TANG, params=None, t_end=0.5, every=1):
+        arr, n = _params_arg(params)
+        added = ctypes.c_int()
+        _check(load().pmhd_learned_generate(self._h, problem, arr, n, t_end, every, ctypes.byref(added)),
+               "pmhd_learned_generate")
+        return added.value
+
+    def train(self, iters=1000, batch=8, lr=2e-3):
+        losses = (ctypes.c_float * iters)()
+        _check(load().pmhd_learned_train(self._h, iters, batch, lr, losses), "pmhd_learned_train")
+        return np.frombuffer(losses, dtype=np.float32).copy()
+
+    def run(self, problem=PROBLEM_ORSZAG_TANG, params=None, t_end=0.5, use_net=True):
+        arr, n = _params_arg(params)
+        out = np.empty((self.cfg.ny, self.cfg.nx, 9), dtype=np.float64)
+        st = LearnedStats()
+        _check(load().pmhd_learned_run(self._h, problem, arr, n, t_end, int(bool(use_net)),
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(st)),
+               "pmhd_learned_run")
+        return out, st
+
+    def fine_run(self, problem=PROBLEM_ORSZAG_TANG, params=None, t_end=0.5, refine=4):
+        arr, n = _params_arg(params)
+        out = np.empty((self.cfg.ny, self.cfg.nx, 9), dtype=np.float64)
+        st = LearnedStats()
+        _check(load().pmhd_learned_fine_run(self._h, problem, arr, n, t_end, refine,
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(st)),
+               "pmhd_learned_fine_run")
+        return out, st
+
+    def save(self, path):
+        _check(load().pmhd_learned_save(self._h, path.encode()), "pmhd_learned_save")
+
+    def load_weights(self, path):
+        _check(load().pmhd_learned_load(self._h, path.encode()), "pmhd_learned_load")
 
 
 def relative_l2(ref, other):

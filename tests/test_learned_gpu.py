@@ -67,7 +67,8 @@ def _wgrad(pmhd, x, dz):
     dw = torch.zeros((co, 9, cin), dtype=torch.float32, device="cuda")
     db = torch.zeros((co,), dtype=torch.float32, device="cuda")
     fp = ctypes.POINTER(ctypes.c_float)
-    rc = pmhd.load().pmhd_conv3x3_wgrad(_dev_bf16(x).data_ptr(), _dev_bf16(dz).data_ptr(), B, H, Wd, cin, co,
+    xd, dzd = _dev_bf16(x), _dev_bf16(dz)  # kept alive across the call
+    rc = pmhd.load().pmhd_conv3x3_wgrad(xd.data_ptr(), dzd.data_ptr(), B, H, Wd, cin, co,
                                         ctypes.cast(dw.data_ptr(), fp), ctypes.cast(db.data_ptr(), fp), None)
     assert rc == pmhd.OK, pmhd.strerror(rc)
     return _host(dw), _host(db)
@@ -173,3 +174,75 @@ def test_unsupported_channel_counts_are_rejected(pmhd_lib):
                                       ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_float)), 24, None,
                                       o.data_ptr(), o.data_ptr(), None)
     assert rc == pmhd_lib.ERR_UNSUPPORTED
+
+
+def test_network_gradient_chain_matches_oracle(pmhd_lib):
+    """The training iteration's chain (forward GELU, GELU, linear; loss
+    gradient; weight gradients; backward through both GELUs) composed from
+    the kernels matches the float64 oracle's analytic gradients."""
+    import torch
+    rng = np.random.default_rng(21)
+    shape = (2, 16, 24)
+    P = shape[0] * shape[1] * shape[2]
+    x = _bf(np.concatenate([rng.normal(0, 1, shape + (18,)), np.zeros(shape + (14,))], axis=3))
+    W1 = _bf(rng.normal(0, 0.1, (32, 9, 32)))
+    W2 = _bf(rng.normal(0, 0.1, (32, 9, 32)))
+    W3 = _bf(rng.normal(0, 0.1, (16, 9, 32)))
+    b1, b2, b3 = (rng.normal(0, 0.05, n).astype(np.float32).astype(np.float64) for n in (32, 32, 16))
+    tgt = rng.normal(0, 1, shape + (16,))
+    tgt[..., 9:] = 0
+    z1, a1 = _conv(pmhd_lib, pmhd_lib.CONV_GELU, x, W1, b1, 32)
+    z2, a2 = _conv(pmhd_lib, pmhd_lib.CONV_GELU, a1, W2, b2, 32)
+    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_LINEAR, a2, W3, b3, 16)
+    d = out - tgt
+    d[..., 9:] = 0
+    dz3 = _bf(2.0 * d / (P * 9))
+    gW3, gb3 = _wgrad(pmhd_lib, a2, dz3)
+    dz2, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz3, np.ascontiguousarray(W3.transpose(2, 1, 0)), None, 32, zprev=z2)
+    gW2, gb2 = _wgrad(pmhd_lib, a1, dz2)
+    dz1, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz2, np.ascontiguousarray(W2.transpose(2, 1, 0)), None, 32, zprev=z1)
+    gW1, gb1 = _wgrad(pmhd_lib, x, dz1)
+    _, grads = C.net_loss_and_grads(x, [(W1, b1), (W2, b2), (W3, b3)], tgt, 9)
+    for (gw, gb), (rw, rb) in zip([(gW1, gb1), (gW2, gb2), (gW3, gb3)], grads):
+        # bf16 activations and gradients: a few per cent of the largest entry.
+        np.testing.assert_allclose(gw, rw, rtol=0, atol=0.03 * np.abs(rw).max())
+        np.testing.assert_allclose(gb, rb, rtol=0, atol=0.03 * np.abs(rb).max())
+        cos = np.sum(gw * rw) / np.sqrt(np.sum(gw * gw) * np.sum(rw * rw))
+        assert cos > 0.999
+
+
+def _rel(a, b):
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+
+
+def test_learned_correction_trains_and_beats_the_plain_coarse_grid(pmhd_lib, tmp_path):
+    """Orszag-Tang with the field scaled by B0: pairs from four training
+    amplitudes (coarse 32^2, fine 128^2), evaluation on a held-out amplitude.
+    The corrected coarse run must be closer to the restricted fine run than
+    the plain coarse run; every correction passes the checks or is counted."""
+    OT = pmhd_lib.PROBLEM_ORSZAG_TANG
+    t_end = 0.2
+    with pmhd_lib.Learned(nx=32, ny=32, refine=4, max_pairs=600, seed=7) as L:
+        for b0 in (0.7, 0.85, 1.15, 1.3):
+            assert L.generate(OT, [b0], t_end=t_end, every=1) > 10
+        losses = L.train(iters=1500, batch=8, lr=2e-3)
+        assert np.all(np.isfinite(losses))
+        assert losses[-100:].mean() < 0.5 * losses[:10].mean()
+        fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=4)
+        plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
+        corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
+        assert sp.t == sc.t == t_end and sp.steps == sc.steps
+        assert sc.accepted + sc.rejected_positivity + sc.rejected_divergence == sc.steps
+        assert sc.accepted > 0
+        e_plain, e_corr = _rel(plain, fine), _rel(corr, fine)
+        print(f"relL2 vs restricted fine: plain {e_plain:.3e} corrected {e_corr:.3e}; "
+              f"accepted {sc.accepted}/{sc.steps}; loss {losses[:10].mean():.3e} -> {losses[-100:].mean():.3e}")
+        assert e_corr < e_plain
+        # Weights and normalisation survive a save / load into a new handle.
+        path = str(tmp_path / "net.bin")
+        L.save(path)
+        with pmhd_lib.Learned(nx=32, ny=32, refine=4, max_pairs=1, seed=99) as L2:
+            L2.load_weights(path)
+            corr2, sc2 = L2.run(OT, [1.0], t_end=t_end, use_net=True)
+            assert sc2.steps == sc.steps
+            np.testing.assert_allclose(corr2, corr, rtol=0, atol=1e-12 * np.abs(corr).max())

@@ -62,3 +62,22 @@ def test_gelu_derivative_matches_finite_differences():
     h = 1e-6
     fd = (C.gelu(z + h) - C.gelu(z - h)) / (2 * h)
     np.testing.assert_allclose(C.gelu_grad(z), fd, atol=1e-8)
+
+
+def test_learned_config_defaults_and_argument_checks(pmhd_lib):
+    import ctypes
+    c = pmhd_lib.LearnedConfig()
+    assert pmhd_lib.load().pmhd_learned_config_default(ctypes.byref(c)) == pmhd_lib.OK
+    assert (c.nx, c.ny, c.refine, c.precision, c.max_pairs) == (64, 64, 4, pmhd_lib.MIXED, 512)
+    h = ctypes.c_void_p(1)
+    bad = pmhd_lib.LearnedConfig.from_buffer_copy(c)
+    bad.refine = 1
+    assert pmhd_lib.load().pmhd_learned_create(ctypes.byref(bad), ctypes.byref(h)) == pmhd_lib.ERR_ARG
+    assert h.value is None
+    bad = pmhd_lib.LearnedConfig.from_buffer_copy(c)
+    bad.precision = pmhd_lib.FP32
+    assert pmhd_lib.load().pmhd_learned_create(ctypes.byref(bad), ctypes.byref(h)) == pmhd_lib.ERR_UNSUPPORTED
+    L = pmhd_lib.load()
+    assert L.pmhd_learned_train(None, 10, 4, 1e-3, None) == pmhd_lib.ERR_ARG
+    assert L.pmhd_learned_destroy(None) == pmhd_lib.OK
+    assert L.pmhd_learned_num_pairs(None) == 0
