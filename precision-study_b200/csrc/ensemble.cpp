@@ -289,8 +289,12 @@ int pmhd_ensemble_create(const pmhd_config* common, const pmhd_member_desc* memb
       rc = PMHD_ERR_NOMEM;
       break;
     }
-    if (cudaMemcpy(e->dTiles[t], tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(e->dTile0[t], tile0.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    // Stream-ordered copies, finished before the host vectors are reused.
+    if (cudaMemcpyAsync(e->dTiles[t], tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, e->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(e->dTile0[t], tile0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
       rc = PMHD_ERR_CUDA;
     Batch& b = e->run.batch[t];
     b.members = e->dMembers;

@@ -35,7 +35,9 @@ int finish(cudaError_t e, int* err, cudaStream_t s) {
     return PMHD_ERR_CUDA;
   }
   int h = 0;
-  if (cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return PMHD_ERR_CUDA;
+  if (cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return PMHD_ERR_CUDA;
   return h ? PMHD_ERR_TIMEOUT : PMHD_OK;
 }
 

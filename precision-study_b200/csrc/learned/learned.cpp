@@ -124,9 +124,13 @@ void fill_stats(pmhd_learned_stats* out, const pmhd_stats& st, double wall_ms) {
   out->status = st.status;
 }
 
-int check_err(pmhd_learned* L) {
+// Every copy and memset below is stream-ordered on the stream whose kernels
+// use the memory: the library's streams are non-blocking, so they are not
+// ordered after the legacy default stream.
+int check_err(pmhd_learned* L, cudaStream_t s) {
   int h = 0;
-  L_CU(cudaMemcpy(&h, L->err, sizeof(int), cudaMemcpyDeviceToHost));
+  L_CU(cudaMemcpyAsync(&h, L->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  L_CU(cudaStreamSynchronize(s));
   return h ? PMHD_ERR_TIMEOUT : PMHD_OK;
 }
 
@@ -227,10 +231,12 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
         }
   }
   int rc = PMHD_OK;
-  if (cudaMemcpy(L->w.theta, th.data(), np * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemset(L->grad, 0, np * sizeof(float)) != cudaSuccess ||
-      cudaMemset(L->m, 0, np * sizeof(float)) != cudaSuccess ||
-      cudaMemset(L->v, 0, np * sizeof(float)) != cudaSuccess || cudaMemset(L->err, 0, sizeof(int)) != cudaSuccess ||
+  cudaStream_t s = L->stream;
+  if (cudaMemcpyAsync(L->w.theta, th.data(), np * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemsetAsync(L->grad, 0, np * sizeof(float), s) != cudaSuccess ||
+      cudaMemsetAsync(L->m, 0, np * sizeof(float), s) != cudaSuccess ||
+      cudaMemsetAsync(L->v, 0, np * sizeof(float), s) != cudaSuccess ||
+      cudaMemsetAsync(L->err, 0, sizeof(int), s) != cudaSuccess ||
       weights_to_bf16(L->L, L->w, L->stream) != cudaSuccess || cudaStreamSynchronize(L->stream) != cudaSuccess)
     rc = PMHD_ERR_CUDA;
   if (rc != PMHD_OK) {
@@ -292,9 +298,10 @@ int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, in
     if (e != cudaSuccess) break;
     if (k % every == 0) {
       const size_t off = (size_t)L->npairs * L->pair_elems;
-      e = cudaMemcpy(L->px + off, cur, bytes, cudaMemcpyDeviceToDevice);
-      if (e == cudaSuccess) e = cudaMemcpy(L->py + off, yy, bytes, cudaMemcpyDeviceToDevice);
-      if (e == cudaSuccess) e = cudaMemcpy(L->pz + off, nxt, bytes, cudaMemcpyDeviceToDevice);
+      e = cudaMemcpyAsync(L->px + off, cur, bytes, cudaMemcpyDeviceToDevice, vf.stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(L->py + off, yy, bytes, cudaMemcpyDeviceToDevice, vf.stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(L->pz + off, nxt, bytes, cudaMemcpyDeviceToDevice, vf.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(vf.stream);
       L->npairs++;
       n_added++;
     }
@@ -349,7 +356,8 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
           L->hnorm.inv_out[k] = lv ? (float)(1.0 / rms) : 0.f;
         }
       }
-    L_CU(cudaMemcpy(L->dnorm, &L->hnorm, sizeof(Norm), cudaMemcpyHostToDevice));
+    L_CU(cudaMemcpyAsync(L->dnorm, &L->hnorm, sizeof(Norm), cudaMemcpyHostToDevice, s));
+    L_CU(cudaStreamSynchronize(s));
     L->have_norm = true;
   }
   // Network inputs and targets of every pair.
@@ -431,7 +439,9 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
     for (int i = 1; e == cudaSuccess && i < iters; i++) e = cudaGraphLaunch(exec, s);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e == cudaSuccess && losses) e = cudaMemcpy(losses, hist, (size_t)iters * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && losses)
+    e = cudaMemcpyAsync(losses, hist, (size_t)iters * sizeof(float), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   release();
@@ -439,7 +449,7 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
     cudaGetLastError();
     return e == cudaErrorNotSupported ? PMHD_ERR_UNSUPPORTED : PMHD_ERR_CUDA;
   }
-  return check_err(L);
+  return check_err(L, s);
 }
 
 int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int use_net,
@@ -479,10 +489,11 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
     return PMHD_ERR_NOMEM;
   }
   cs.norm = L->dnorm;
-  cudaError_t e = cudaMemset(cs.flags, 0, 4 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(cs.sums, 0, 4 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemset(cs.counters, 0, 4 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemset(L->err, 0, sizeof(int));
+  cudaError_t e = cudaMemsetAsync(cs.flags, 0, 4 * sizeof(int), vc.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cs.sums, 0, 4 * sizeof(double), vc.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cs.counters, 0, 4 * sizeof(unsigned long long), vc.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L->err, 0, sizeof(int), vc.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(vc.stream);
   if (e != cudaSuccess) {
     release();
     return PMHD_ERR_CUDA;
@@ -536,14 +547,15 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
   }
   if (rc == PMHD_OK && use_net && stats) {
     unsigned long long h[4];
-    if (cudaMemcpy(h, cs.counters, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
+    if (cudaMemcpyAsync(h, cs.counters, sizeof(h), cudaMemcpyDeviceToHost, vc.stream) == cudaSuccess &&
+        cudaStreamSynchronize(vc.stream) == cudaSuccess) {
       stats->accepted = (long long)h[0];
       stats->rejected_positivity = (long long)h[1];
       stats->rejected_divergence = (long long)h[2];
     }
   }
   if (use_net) solver_set_step_hooks(c.s, nullptr, nullptr);
-  if (rc == PMHD_OK) rc = check_err(L);
+  if (rc == PMHD_OK) rc = check_err(L, vc.stream);
   release();
   return rc;
 }
@@ -580,7 +592,9 @@ int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, in
 int pmhd_learned_save(const pmhd_learned* L, const char* path) {
   if (!L || !path || !L->have_norm) return PMHD_ERR_ARG;
   std::vector<float> th(L->L.n_params);
-  if (cudaMemcpy(th.data(), L->w.theta, th.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(th.data(), L->w.theta, th.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(L->stream) != cudaSuccess)
     return PMHD_ERR_CUDA;
   FILE* f = std::fopen(path, "wb");
   if (!f) return PMHD_ERR_IO;
@@ -608,8 +622,8 @@ int pmhd_learned_load(pmhd_learned* L, const char* path) {
   L_CU(cudaSetDevice(L->cfg.device));
   L->hnorm = nm;
   L->have_norm = true;
-  L_CU(cudaMemcpy(L->dnorm, &nm, sizeof(Norm), cudaMemcpyHostToDevice));
-  L_CU(cudaMemcpy(L->w.theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice));
+  L_CU(cudaMemcpyAsync(L->dnorm, &nm, sizeof(Norm), cudaMemcpyHostToDevice, L->stream));
+  L_CU(cudaMemcpyAsync(L->w.theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice, L->stream));
   L_CU(weights_to_bf16(L->L, L->w, L->stream));
   L_CU(cudaStreamSynchronize(L->stream));
   return PMHD_OK;

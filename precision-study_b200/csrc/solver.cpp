@@ -261,7 +261,9 @@ int pmhd_create(const pmhd_config* cfg, pmhd_solver** out) {
     set_member_physics(m, cfg->x_min, cfg->x_max, cfg->y_min, cfg->y_max, cfg->gamma, cfg->hlld_tol, cfg->cfl,
                        cfg->alpha, cfg->order == PMHD_ORDER_MUSCL ? 1 : 0, cfg->bc, is_fp32(s));
     if (!encode_member_tmaps(m, s->elem)) rc = PMHD_ERR_CUDA;
-    if (rc == PMHD_OK && cudaMemcpy(s->dMember, &m, sizeof(m), cudaMemcpyHostToDevice) != cudaSuccess)
+    // Stream-ordered (the solver's stream does not wait for the legacy stream).
+    if (rc == PMHD_OK && (cudaMemcpyAsync(s->dMember, &m, sizeof(m), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+                          cudaStreamSynchronize(s->stream) != cudaSuccess))
       rc = PMHD_ERR_CUDA;
     s->hMember = m;
     s->run.single = &s->hMember;

@@ -231,7 +231,7 @@ def test_learned_correction_trains_and_beats_the_plain_coarse_grid(pmhd_lib, tmp
         fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=4)
         plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
         corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
-        assert sp.t == sc.t == t_end and sp.steps == sc.steps
+        assert sp.t == sc.t == t_end  # the corrected run's CFL steps differ slightly
         assert sc.accepted + sc.rejected_positivity + sc.rejected_divergence == sc.steps
         assert sc.accepted > 0
         e_plain, e_corr = _rel(plain, fine), _rel(corr, fine)
