@@ -193,6 +193,48 @@ def time_precision(pmhd, precision, n, warmup, steps, device, sampler=None):
     return s, st, launches
 
 
+def bench_learned(pmhd, n, device, refine=4, t_end=0.25):
+    """Learned correction of the Orszag-Tang family (field scaled by B0):
+    training pairs from four amplitudes on the n^2 coarse / (refine n)^2 fine
+    grids, evaluation on the held-out B0 = 1.  Errors are relative L2 (mean
+    over the seven non-trivial variables, and rho) against the fine run
+    restricted to the coarse grid; wall times are those of the time loops."""
+    import numpy as np
+    OT = pmhd.PROBLEM_ORSZAG_TANG
+    live = [0, 1, 2, 4, 5, 6, 8]  # rho, mx, my, E, Bx, By, psi (mz = Bz = 0 in 2D OT)
+
+    def err(a, ref):
+        r = pmhd.relative_l2(ref, a)
+        return {"rho": float(r[0]), "mean": float(np.mean([r[k] for k in live if k != 8]))}
+
+    out = {"coarse": n, "fine": refine * n, "problem": "Orszag-Tang, B0 in {0.7,0.85,1.15,1.3} train, B0=1 test",
+           "t_end": t_end}
+    with pmhd.Learned(nx=n, ny=n, refine=refine, max_pairs=640, seed=11, device=device) as L:
+        t0 = time.perf_counter()
+        for b0 in (0.7, 0.85, 1.15, 1.3):
+            L.generate(OT, [b0], t_end=t_end, every=2)
+        t1 = time.perf_counter()
+        losses = L.train(iters=1500, batch=8, lr=2e-3)
+        t2 = time.perf_counter()
+        fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=refine)
+        plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
+        corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
+        two, s2 = L.fine_run(OT, [1.0], t_end=t_end, refine=2)
+        out.update({
+            "pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": 1500,
+            "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-100:].mean()),
+            "relL2_vs_fine": {"plain_coarse": err(plain, fine), "learned_coarse": err(corr, fine),
+                              "plain_2x": err(two, fine)},
+            "wall_ms": {"fine": sf.wall_ms, "plain_coarse": sp.wall_ms, "learned_coarse": sc.wall_ms,
+                        "plain_2x": s2.wall_ms},
+            "steps": {"fine": sf.steps, "plain_coarse": sp.steps, "learned_coarse": sc.steps, "plain_2x": s2.steps},
+            "corrections": {"accepted": sc.accepted, "rejected_positivity": sc.rejected_positivity,
+                            "rejected_divergence": sc.rejected_divergence},
+            "speedup_vs_fine_wall": sf.wall_ms / sc.wall_ms,
+        })
+    return out
+
+
 def bench_ensemble(pmhd, nmem, seed, prec, W, K, device, barrier, max_over_ranks, world):
     """Zone-cycles/s of the seeded uneven ensemble (square grids from
     {64,128,256,512}, half Orszag-Tang with scaled field, half Brio-Wu bands
@@ -244,6 +286,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
     ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
     ap.add_argument("--ensemble-seed", type=int, default=2024)
+    ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -353,6 +396,11 @@ def main():
         ens = bench_ensemble(pmhd, args.ensemble, args.ensemble_seed, prec, W, K, local, barrier, max_over_ranks,
                              world)
 
+    # ---- learned coarse-grid correction: accuracy and wall time ---------------
+    learned = None
+    if args.learned > 0 and rank == 0:
+        learned = bench_learned(pmhd, args.learned, local)
+
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -381,6 +429,8 @@ def main():
         line.update(extra)
         if ens is not None:
             line["ensemble"] = ens
+        if learned is not None:
+            line["learned"] = learned
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
