@@ -62,7 +62,7 @@ typedef enum {
 typedef enum { PMHD_FP64 = 0, PMHD_FP32 = 1, PMHD_MIXED = 2 } pmhd_precision;
 typedef enum { PMHD_BC_PERIODIC = 0, PMHD_BC_REFLECT = 1, PMHD_BC_TRANSMISSIVE = 2 } pmhd_bc;
 typedef enum { PMHD_ORDER_FIRST = 0, PMHD_ORDER_MUSCL = 1 } pmhd_order;
-typedef enum { PMHD_SOLVER_HLL = 0, PMHD_SOLVER_HLLD = 1 } pmhd_solver_kind;
+typedef enum { PMHD_SOLVER_HLL = 0, PMHD_SOLVER_HLLD = 1, PMHD_SOLVER_HLLC = 2 /* Euler */ } pmhd_solver_kind;
 typedef enum {
   PMHD_PROBLEM_ORSZAG_TANG = 0, /* mhd2d_glm_gpu.cu:443-451, unit periodic box        */
   PMHD_PROBLEM_KH_REF = 1,      /* the reference's doubly periodic double shear layer */
@@ -327,6 +327,39 @@ int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, in
 /* Network weights and normalisation to / from a file. */
 int pmhd_learned_save(const pmhd_learned* L, const char* path);
 int pmhd_learned_load(pmhd_learned* L, const char* path);
+
+/* ---- Euler sibling (gamma = 1.4) -------------------------------------------------
+ * The reference's 1D and 2D MUSCL-Hancock + HLLC / HLL Euler programs
+ * (src/euler/riemann1d_cpu.cpp, src/euler/riemann2d_cpu.cpp): same problems,
+ * CFL 0.8, transmissive walls, dimensionally split 2D steps alternating x-y
+ * and y-x.  solver: PMHD_SOLVER_HLLC or PMHD_SOLVER_HLL; precision:
+ * PMHD_FP64 or PMHD_FP32; exact = 1 gives the reference CPU build's bits. */
+typedef struct pmhd_euler2d pmhd_euler2d;
+
+typedef struct {
+  long long steps;
+  double t;
+  double device_ms;    /* device time of the steps of this call */
+  int status;
+} pmhd_euler_stats;
+
+/* nx x ny grid on [0,1]^2 holding Liska-Wendroff configuration `config`
+ * (3, 6 or 12; riemann2d_cpu.cpp:54-76). */
+int pmhd_euler2d_create(int nx, int ny, int config, int solver, int precision, int exact, int device,
+                        pmhd_euler2d** out);
+/* Advances until t_end (< 0: the configuration's end time) or max_steps
+ * steps (< 0: no limit). */
+int pmhd_euler2d_advance(pmhd_euler2d* e, double t_end, long long max_steps, pmhd_euler_stats* stats);
+/* Primitive state (rho, u, v, p) of the interior, [ny][nx][4] values of the
+ * precision's type. */
+int pmhd_euler2d_get_prim(pmhd_euler2d* e, void* host);
+int pmhd_euler2d_destroy(pmhd_euler2d* e);
+
+/* Toro test `test` (1-5; riemann1d_cpu.cpp:43-62) on n cells of [0,1] to its
+ * end time, in one kernel launch; host_out (may be NULL): [n][3] = rho, u, p
+ * of the precision's type, as the reference writes them. */
+int pmhd_euler1d_run(int n, int test, int solver, int precision, int exact, int device, void* host_out,
+                     pmhd_euler_stats* stats);
 
 /* ---- Allocation-free time loop ----------------------------------------------
  * No counterpart in the reference: its program always cudaMallocs five state

@@ -186,12 +186,14 @@ static int EN(eo_lw_config)(int id, ET q[4][4], ET* t_end) {
   return 1;
 }
 
-/* 2D Riemann problem, N x N on [0,1]^2, CFL 0.8, transmissive walls
- * (riemann2d_cpu.cpp:108-330).  max_steps < 0: run to T_end (t_end < 0:
- * the configuration's).  out: primitive interior [N][N][4] (rho, u, v, p).
- * Returns the step count, or -1 on a bad configuration / allocation. */
-long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long max_steps, ET* out, ET* t_out) {
-  const int GH = 2, TX = N + 4, TY = N + 4;
+/* 2D Riemann problem, NX x NY on [0,1]^2 (the reference runs N x N), CFL
+ * 0.8, transmissive walls (riemann2d_cpu.cpp:108-330).  max_steps < 0: run
+ * to T_end (t_end < 0: the configuration's).  out: primitive interior
+ * [NY][NX][4] (rho, u, v, p).  Returns the step count, or -1 on a bad
+ * configuration / allocation. */
+long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, long long max_steps, ET* out,
+                           ET* t_out) {
+  const int GH = 2, TX = NX + 4, TY = NY + 4;
   const size_t SZ = (size_t)TX * TY;
   ET q[4][4], T_end;
   ET *rho, *ru, *rv, *E, *W[4], *WL[4], *WR[4], *WLh[4], *WRh[4], *F[4];
@@ -199,8 +201,8 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
   int i, j, k, g;
   long long step = 0;
   ET t = (ET)0.0;
-  const ET dx = ((ET)1.0 - (ET)0.0) / (ET)N, dy = ((ET)1.0 - (ET)0.0) / (ET)N, cfl = (ET)0.8;
-  if (!EN(eo_lw_config)(cfg_id, q, &T_end) || N < 2) return -1;
+  const ET dx = ((ET)1.0 - (ET)0.0) / (ET)NX, dy = ((ET)1.0 - (ET)0.0) / (ET)NY, cfl = (ET)0.8;
+  if (!EN(eo_lw_config)(cfg_id, q, &T_end) || NX < 2 || NY < 2) return -1;
   if (t_end_in > (ET)0.0) T_end = t_end_in;
   blk = (ET*)calloc(SZ * 24, sizeof(ET));
   if (!blk) return -1;
@@ -226,7 +228,7 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
   }
 #define BC()                                                                                   \
   do {                                                                                         \
-    for (j = GH; j < N + GH; j++)                                                              \
+    for (j = GH; j < NY + GH; j++)                                                              \
       for (g = 0; g < GH; g++) {                                                               \
         size_t gL = ID(g, j), iL = ID(GH, j), gR = ID(TX - 1 - g, j), iR = ID(TX - 1 - GH, j); \
         rho[gL] = rho[iL]; ru[gL] = ru[iL]; rv[gL] = rv[iL]; E[gL] = E[iL];                    \
@@ -252,8 +254,8 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
     ET mx = (ET)0, my = (ET)0, dt;
     int pass;
     C2P();
-    for (j = GH; j < N + GH; j++)
-      for (i = GH; i < N + GH; i++) {
+    for (j = GH; j < NY + GH; j++)
+      for (i = GH; i < NX + GH; i++) {
         size_t id = ID(i, j);
         ET c = EN(eo_sound)(W[3][id], W[0][id]);
         mx = EN(eo_max)(mx, (ET)fabs(W[1][id]) + c);
@@ -267,12 +269,12 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
       if (pass == 1) C2P();
       if (xsweep) {
         ET fac = (ET)0.5 * dt / dx, rx = dt / dx;
-        for (j = GH; j < N + GH; j++)
+        for (j = GH; j < NY + GH; j++)
           for (i = 1; i < TX - 1; i++) {
             size_t id = ID(i, j), a = ID(i - 1, j), b = ID(i + 1, j);
             for (k = 0; k < 4; k++) EN(eo_recon)(W[k][a], W[k][id], W[k][b], &WL[k][id], &WR[k][id]);
           }
-        for (j = GH; j < N + GH; j++)
+        for (j = GH; j < NY + GH; j++)
           for (i = 1; i < TX - 1; i++) {
             size_t id = ID(i, j);
             ET l[4] = {WL[0][id], WL[1][id], WL[2][id], WL[3][id]}, r[4] = {WR[0][id], WR[1][id], WR[2][id], WR[3][id]};
@@ -281,16 +283,16 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
             EN(eo_hancock)(r, l, r, rh, fac, 1, 2);
             for (k = 0; k < 4; k++) { WLh[k][id] = lh[k]; WRh[k][id] = rh[k]; }
           }
-        for (j = GH; j < N + GH; j++)
-          for (i = GH - 1; i < N + GH; i++) {
+        for (j = GH; j < NY + GH; j++)
+          for (i = GH - 1; i < NX + GH; i++) {
             size_t a = ID(i, j), b = ID(i + 1, j);
             ET l[4] = {WRh[0][a], WRh[1][a], WRh[2][a], WRh[3][a]}, r[4] = {WLh[0][b], WLh[1][b], WLh[2][b], WLh[3][b]};
             ET f[4];
             if (hll) EN(eo_hll)(l, r, f, 1, 2); else EN(eo_hllc)(l, r, f, 1, 2);
             for (k = 0; k < 4; k++) F[k][a] = f[k];
           }
-        for (j = GH; j < N + GH; j++)
-          for (i = GH; i < N + GH; i++) {
+        for (j = GH; j < NY + GH; j++)
+          for (i = GH; i < NX + GH; i++) {
             size_t id = ID(i, j), il = ID(i - 1, j);
             rho[id] -= rx * (F[0][id] - F[0][il]);
             ru[id] -= rx * (F[1][id] - F[1][il]);
@@ -300,12 +302,12 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
       } else {
         ET fac = (ET)0.5 * dt / dy, ry = dt / dy;
         for (j = 1; j < TY - 1; j++)
-          for (i = GH; i < N + GH; i++) {
+          for (i = GH; i < NX + GH; i++) {
             size_t id = ID(i, j), a = ID(i, j - 1), b = ID(i, j + 1);
             for (k = 0; k < 4; k++) EN(eo_recon)(W[k][a], W[k][id], W[k][b], &WL[k][id], &WR[k][id]);
           }
         for (j = 1; j < TY - 1; j++)
-          for (i = GH; i < N + GH; i++) {
+          for (i = GH; i < NX + GH; i++) {
             size_t id = ID(i, j);
             ET l[4] = {WL[0][id], WL[1][id], WL[2][id], WL[3][id]}, r[4] = {WR[0][id], WR[1][id], WR[2][id], WR[3][id]};
             ET lh[4], rh[4];
@@ -313,16 +315,16 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
             EN(eo_hancock)(r, l, r, rh, fac, 2, 1);
             for (k = 0; k < 4; k++) { WLh[k][id] = lh[k]; WRh[k][id] = rh[k]; }
           }
-        for (j = GH - 1; j < N + GH; j++)
-          for (i = GH; i < N + GH; i++) {
+        for (j = GH - 1; j < NY + GH; j++)
+          for (i = GH; i < NX + GH; i++) {
             size_t a = ID(i, j), b = ID(i, j + 1);
             ET l[4] = {WRh[0][a], WRh[1][a], WRh[2][a], WRh[3][a]}, r[4] = {WLh[0][b], WLh[1][b], WLh[2][b], WLh[3][b]};
             ET f[4];
             if (hll) EN(eo_hll)(l, r, f, 2, 1); else EN(eo_hllc)(l, r, f, 2, 1);
             for (k = 0; k < 4; k++) F[k][a] = f[k];
           }
-        for (j = GH; j < N + GH; j++)
-          for (i = GH; i < N + GH; i++) {
+        for (j = GH; j < NY + GH; j++)
+          for (i = GH; i < NX + GH; i++) {
             size_t id = ID(i, j), ib = ID(i, j - 1);
             rho[id] -= ry * (F[0][id] - F[0][ib]);
             ru[id] -= ry * (F[1][id] - F[1][ib]);
@@ -336,9 +338,9 @@ long long EN(eo_riemann2d)(int N, int cfg_id, int hll, ET t_end_in, long long ma
     step++;
   }
   C2P();
-  for (j = 0; j < N; j++)
-    for (i = 0; i < N; i++)
-      for (k = 0; k < 4; k++) out[((size_t)j * N + i) * 4 + k] = W[k][ID(i + GH, j + GH)];
+  for (j = 0; j < NY; j++)
+    for (i = 0; i < NX; i++)
+      for (k = 0; k < 4; k++) out[((size_t)j * NX + i) * 4 + k] = W[k][ID(i + GH, j + GH)];
   if (t_out) *t_out = t;
 #undef BC
 #undef C2P

@@ -26,7 +26,7 @@ ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE = -1, -2, -3, -4
 FP64, FP32, MIXED = 0, 1, 2
 BC_PERIODIC, BC_REFLECT, BC_TRANSMISSIVE = 0, 1, 2
 ORDER_FIRST, ORDER_MUSCL = 0, 1
-SOLVER_HLL, SOLVER_HLLD = 0, 1
+SOLVER_HLL, SOLVER_HLLD, SOLVER_HLLC = 0, 1, 2
 PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D, PROBLEM_BRIO_WU_TORUS = 0, 1, 2, 3, 4
 LAYOUT_INTERIOR, LAYOUT_GHOSTED = 0, 1
 CONV_GELU, CONV_LINEAR, CONV_DGELU = 0, 1, 2
@@ -45,6 +45,8 @@ EXPORTS = (
     "pmhd_learned_config_default", "pmhd_learned_create", "pmhd_learned_destroy", "pmhd_learned_generate",
     "pmhd_learned_num_pairs", "pmhd_learned_train", "pmhd_learned_run", "pmhd_learned_fine_run",
     "pmhd_learned_save", "pmhd_learned_load",
+    "pmhd_euler2d_create", "pmhd_euler2d_advance", "pmhd_euler2d_get_prim", "pmhd_euler2d_destroy",
+    "pmhd_euler1d_run",
 )
 
 
@@ -126,6 +128,12 @@ class LearnedStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class EulerStats(ctypes.Structure):
+    """pmhd_euler_stats."""
+    _fields_ = [("steps", ctypes.c_longlong), ("t", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("status", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -173,6 +181,11 @@ def load():
         "pmhd_learned_fine_run": ([vp, i, P(d), i, d, i, P(d), P(LearnedStats)], i),
         "pmhd_learned_save": ([vp, ctypes.c_char_p], i),
         "pmhd_learned_load": ([vp, ctypes.c_char_p], i),
+        "pmhd_euler2d_create": ([i, i, i, i, i, i, i, P(vp)], i),
+        "pmhd_euler2d_advance": ([vp, d, ctypes.c_longlong, P(EulerStats)], i),
+        "pmhd_euler2d_get_prim": ([vp, vp], i),
+        "pmhd_euler2d_destroy": ([vp], i),
+        "pmhd_euler1d_run": ([i, i, i, i, i, i, vp, P(EulerStats)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -484,6 +497,60 @@ class Learned:
 
     def load_weights(self, path):
         _check(load().pmhd_learned_load(self._h, path.encode()), "pmhd_learned_load")
+
+
+def _euler_solver(solver):
+    return SOLVER_HLL if solver == "hll" else SOLVER_HLLC
+
+
+class Euler2D:
+    """The Euler sibling's 2D Riemann problem (a pmhd_euler2d handle):
+    Liska-Wendroff configuration 3, 6 or 12 on an nx x ny grid."""
+
+    def __init__(self, nx, ny=None, config=3, solver="hllc", precision="fp64", exact=False, device=0):
+        ny = nx if ny is None else ny
+        self.nx, self.ny = nx, ny
+        self.dtype = np.float32 if precision == "fp32" else np.float64
+        h = ctypes.c_void_p()
+        _check(load().pmhd_euler2d_create(nx, ny, config, _euler_solver(solver), PRECISIONS[precision],
+                                          int(bool(exact)), device, ctypes.byref(h)), "pmhd_euler2d_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pmhd_euler2d_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, t_end=-1.0, max_steps=-1):
+        st = EulerStats()
+        _check(load().pmhd_euler2d_advance(self._h, t_end, max_steps, ctypes.byref(st)), "pmhd_euler2d_advance")
+        return st
+
+    def prims(self):
+        out = np.empty((self.ny, self.nx, 4), dtype=self.dtype)
+        _check(load().pmhd_euler2d_get_prim(self._h, out.ctypes.data), "pmhd_euler2d_get_prim")
+        return out
+
+
+def euler1d(n, test, solver="hllc", precision="fp64", exact=False, device=0):
+    """Toro test `test` on n cells: (EulerStats, [n][3] = rho, u, p)."""
+    out = np.empty((n, 3), dtype=np.float32 if precision == "fp32" else np.float64)
+    st = EulerStats()
+    _check(load().pmhd_euler1d_run(n, test, _euler_solver(solver), PRECISIONS[precision], int(bool(exact)), device,
+                                   out.ctypes.data, ctypes.byref(st)), "pmhd_euler1d_run")
+    return st, out
 
 
 def relative_l2(ref, other):

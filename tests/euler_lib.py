@@ -22,15 +22,17 @@ def _np(prec):
     return np.float64 if prec == "fp64" else np.float32
 
 
-def riemann2d(n, config, solver="hllc", prec="fp64", t_end=-1.0, max_steps=-1):
-    """Oracle 2D Riemann run: (steps, t, prims [n][n][4])."""
+def riemann2d(n, config, solver="hllc", prec="fp64", t_end=-1.0, max_steps=-1, ny=None):
+    """Oracle 2D Riemann run on n x ny (default n x n): (steps, t, prims [ny][n][4])."""
     T = _ctype(prec)
+    ny = n if ny is None else ny
     fn = getattr(_lib(), "eo_riemann2d_" + ("f64" if prec == "fp64" else "f32"))
     fn.restype = ctypes.c_longlong
-    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, T, ctypes.c_longlong, ctypes.c_void_p, ctypes.POINTER(T)]
-    out = np.zeros((n, n, 4), dtype=_np(prec))
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, T, ctypes.c_longlong, ctypes.c_void_p,
+                   ctypes.POINTER(T)]
+    out = np.zeros((ny, n, 4), dtype=_np(prec))
     t = T()
-    steps = fn(n, config, 1 if solver == "hll" else 0, T(t_end), max_steps, out.ctypes.data, ctypes.byref(t))
+    steps = fn(n, ny, config, 1 if solver == "hll" else 0, T(t_end), max_steps, out.ctypes.data, ctypes.byref(t))
     assert steps >= 0
     return steps, t.value, out
 

@@ -1,0 +1,74 @@
+"""GPU checks of the Euler sibling (pmhd_euler2d_*, pmhd_euler1d_run).
+
+Exact build: every golden run of the reference's 1D and 2D programs
+(tests/golden/euler_runs.json) is reproduced bit for bit (md5 of the .dat
+the reference would write) and so is the oracle on rectangular grids with
+partial tiles and on step-limited, resumed runs.  Fast build: within
+rounding-level tolerances of the oracle.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import euler_lib as EL
+
+pytestmark = pytest.mark.gpu
+GOLD = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "euler_runs.json")))
+
+
+@pytest.mark.parametrize("run", GOLD["runs2d"], ids=lambda r: f"{r['n']}-cfg{r['config']}-{r['solver']}-{r['precision']}")
+def test_2d_exact_reproduces_the_reference(pmhd_lib, run):
+    with pmhd_lib.Euler2D(run["n"], config=run["config"], solver=run["solver"], precision=run["precision"],
+                          exact=True) as e:
+        st = e.advance()
+        assert st.steps == run["steps"]
+        assert EL.dat_md5_2d(e.prims(), run["precision"]) == run["md5"]
+
+
+@pytest.mark.parametrize("run", GOLD["runs1d"], ids=lambda r: f"toro{r['test']}-{r['solver']}-{r['precision']}")
+def test_1d_exact_reproduces_the_reference(pmhd_lib, run):
+    st, out = pmhd_lib.euler1d(run["n"], run["test"], run["solver"], run["precision"], exact=True)
+    assert st.steps == run["steps"]
+    assert EL.dat_md5_1d(out, run["precision"]) == run["md5"]
+
+
+@pytest.mark.parametrize("shape", [(100, 70), (33, 47), (17, 129)])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_2d_exact_rectangular_grids_match_the_oracle(oracle, pmhd_lib, shape, prec):
+    nx, ny = shape
+    steps, t, ref = EL.riemann2d(nx, 6, "hllc", prec, ny=ny)
+    with pmhd_lib.Euler2D(nx, ny, config=6, precision=prec, exact=True) as e:
+        st = e.advance()
+        assert st.steps == steps
+        np.testing.assert_array_equal(e.prims(), ref)
+
+
+def test_2d_step_limited_runs_resume_exactly(oracle, pmhd_lib):
+    steps, t, ref = EL.riemann2d(80, 12, "hllc", "fp64")
+    _, _, ref7 = EL.riemann2d(80, 12, "hllc", "fp64", max_steps=7)
+    with pmhd_lib.Euler2D(80, config=12, exact=True) as e:
+        assert e.advance(max_steps=7).steps == 7
+        np.testing.assert_array_equal(e.prims(), ref7)
+        assert e.advance().steps == steps
+        np.testing.assert_array_equal(e.prims(), ref)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 1e-4)])
+@pytest.mark.parametrize("config", [3, 6, 12])
+def test_2d_fast_build_close_to_the_oracle(oracle, pmhd_lib, prec, tol, config):
+    _, _, ref = EL.riemann2d(128, config, "hllc", prec)
+    with pmhd_lib.Euler2D(128, config=config, precision=prec, exact=False) as e:
+        e.advance()
+        got = e.prims().astype(np.float64)
+    rel = pmhd_lib.relative_l2(ref.astype(np.float64), got)
+    assert np.all(rel < tol), rel
+
+
+@pytest.mark.parametrize("test", [1, 2, 3, 4, 5])
+def test_1d_fast_build_close_to_the_oracle(oracle, pmhd_lib, test):
+    _, _, ref = EL.riemann1d(400, test, "hllc", "fp64")
+    st, out = pmhd_lib.euler1d(400, test, "hllc", "fp64", exact=False)
+    rel = pmhd_lib.relative_l2(ref, out)
+    assert np.all(rel < 1e-10), rel
