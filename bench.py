@@ -193,6 +193,28 @@ def time_precision(pmhd, precision, n, warmup, steps, device, sampler=None):
     return s, st, launches
 
 
+def bench_euler(pmhd, n, W, K, device, max_over_ranks, world):
+    """Zone-cycles/s of the Euler sibling's 2D step (Liska-Wendroff
+    configuration 3, HLLC, fused x/y sweeps) at n^2, fp64 and fp32.  A step
+    reads and writes the 4 conservative planes once: 64 B/cell (fp64), 32 B
+    (fp32) of algorithmic HBM traffic."""
+    peak, _ = measured_peaks()
+    out = {"grid": n, "problem": "Liska-Wendroff configuration 3, MUSCL-Hancock + HLLC, split x/y",
+           "algorithmic_bytes_per_cell_step": {"fp64": 64, "fp32": 32}}
+    for prec in ("fp64", "fp32"):
+        with pmhd.Euler2D(n, config=3, precision=prec, device=device) as e:
+            e.advance(max_steps=W + (W & 1))
+            st = e.advance(max_steps=K + (K & 1))
+            ms = max_over_ranks(st.device_ms)
+            steps = K + (K & 1)
+            value = world * n * n * steps / (ms / 1e3)
+            bpc = 64 if prec == "fp64" else 32
+            gbs = bpc * n * n * steps / (ms / 1e3) / 1e9
+            out[prec] = {"value": value, "unit": UNIT, "ms_per_step": ms / steps,
+                         "roofline": {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}}
+    return out
+
+
 def bench_learned(pmhd, n, device, refine=4, t_end=0.25):
     """Learned correction of the Orszag-Tang family (field scaled by B0):
     training pairs from four amplitudes on the n^2 coarse / (refine n)^2 fine
@@ -287,6 +309,7 @@ def main():
     ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
     ap.add_argument("--ensemble-seed", type=int, default=2024)
     ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
+    ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -396,6 +419,11 @@ def main():
         ens = bench_ensemble(pmhd, args.ensemble, args.ensemble_seed, prec, W, K, local, barrier, max_over_ranks,
                              world)
 
+    # ---- Euler sibling: fused split steps of the 2D Riemann problem ----------
+    euler = None
+    if args.euler > 0:
+        euler = bench_euler(pmhd, args.euler, W, K, local, max_over_ranks, world)
+
     # ---- learned coarse-grid correction: accuracy and wall time ---------------
     learned = None
     if args.learned > 0 and rank == 0:
@@ -431,6 +459,8 @@ def main():
             line["ensemble"] = ens
         if learned is not None:
             line["learned"] = learned
+        if euler is not None:
+            line["euler2d"] = euler
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
