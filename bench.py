@@ -215,7 +215,7 @@ def bench_euler(pmhd, n, W, K, device, max_over_ranks, world):
     return out
 
 
-def bench_learned(pmhd, n, device, refine=4, t_end=0.25):
+def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500):
     """Learned correction of the Orszag-Tang family (field scaled by B0):
     training pairs from four amplitudes on the n^2 coarse / (refine n)^2 fine
     grids, evaluation on the held-out B0 = 1.  Errors are relative L2 (mean
@@ -236,14 +236,18 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25):
         for b0 in (0.7, 0.85, 1.15, 1.3):
             L.generate(OT, [b0], t_end=t_end, every=2)
         t1 = time.perf_counter()
-        losses = L.train(iters=1500, batch=8, lr=2e-3)
+        losses = L.train(iters=iters, batch=8, lr=2e-3)
         t2 = time.perf_counter()
         fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=refine)
         plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
-        corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
         two, s2 = L.fine_run(OT, [1.0], t_end=t_end, refine=2)
+        try:
+            corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
+        except pmhd.PmhdError as exc:  # a corrected state the solver could not advance
+            out.update({"pairs": L.num_pairs, "corrected_run": f"failed: {exc}"})
+            return out
         out.update({
-            "pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": 1500,
+            "pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": iters,
             "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-100:].mean()),
             "relL2_vs_fine": {"plain_coarse": err(plain, fine), "learned_coarse": err(corr, fine),
                               "plain_2x": err(two, fine)},
@@ -309,6 +313,7 @@ def main():
     ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
     ap.add_argument("--ensemble-seed", type=int, default=2024)
     ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
+    ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
     ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -427,7 +432,7 @@ def main():
     # ---- learned coarse-grid correction: accuracy and wall time ---------------
     learned = None
     if args.learned > 0 and rank == 0:
-        learned = bench_learned(pmhd, args.learned, local)
+        learned = bench_learned(pmhd, args.learned, local, iters=args.learned_iters)
 
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
     cpu = None
