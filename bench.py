@@ -315,6 +315,7 @@ def main():
     ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
     ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
     ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
+    ap.add_argument("--hancock", type=int, default=4096, help="grid of the MUSCL-Hancock line (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -424,6 +425,24 @@ def main():
         ens = bench_ensemble(pmhd, args.ensemble, args.ensemble_seed, prec, W, K, local, barrier, max_over_ranks,
                              world)
 
+    # ---- MUSCL-Hancock variant: one stage per step ----------------------------
+    hancock = None
+    if args.hancock > 0:
+        hancock = {"grid": args.hancock, "workload": f"Orszag-Tang {args.hancock}^2, MUSCL-Hancock + HLLD + GLM",
+                   "algorithmic_bytes_per_zone_cycle": {"fp64": 144, "fp32": 72}}
+        for hp in ("fp64", "fp32"):
+            sh = pmhd.Solver(nx=args.hancock, ny=args.hancock, precision=hp, order="hancock", device=local)
+            sh.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
+            sh.advance(max_steps=W + (W & 1))
+            sth = sh.advance(max_steps=K + (K & 1))
+            sh.close()
+            msh = max_over_ranks(sth.device_ms)
+            nst = K + (K & 1)
+            bpc = 144 if hp == "fp64" else 72
+            hancock[hp] = {"value": world * args.hancock ** 2 * nst / (msh / 1e3), "unit": UNIT,
+                           "ms_per_step": msh / nst,
+                           "achieved_GBs": bpc * args.hancock ** 2 * nst / (msh / 1e3) / 1e9}
+
     # ---- Euler sibling: fused split steps of the 2D Riemann problem ----------
     euler = None
     if args.euler > 0:
@@ -466,6 +485,8 @@ def main():
             line["learned"] = learned
         if euler is not None:
             line["euler2d"] = euler
+        if hancock is not None:
+            line["hancock"] = hancock
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -61,7 +61,11 @@ typedef enum {
 
 typedef enum { PMHD_FP64 = 0, PMHD_FP32 = 1, PMHD_MIXED = 2 } pmhd_precision;
 typedef enum { PMHD_BC_PERIODIC = 0, PMHD_BC_REFLECT = 1, PMHD_BC_TRANSMISSIVE = 2 } pmhd_bc;
-typedef enum { PMHD_ORDER_FIRST = 0, PMHD_ORDER_MUSCL = 1 } pmhd_order;
+/* PMHD_ORDER_HANCOCK: MUSCL reconstruction + Hancock half-step predictor, one
+ * stage per step (no counterpart in the reference's 2D program; the 2D form
+ * of its 1D predictor, src/mhd/mhd1d_cpu.cpp:203-235).  fp64 / fp32 only;
+ * single grids only (not ensembles or pmhd_advance_noalloc). */
+typedef enum { PMHD_ORDER_FIRST = 0, PMHD_ORDER_MUSCL = 1, PMHD_ORDER_HANCOCK = 2 } pmhd_order;
 typedef enum { PMHD_SOLVER_HLL = 0, PMHD_SOLVER_HLLD = 1, PMHD_SOLVER_HLLC = 2 /* Euler */ } pmhd_solver_kind;
 typedef enum {
   PMHD_PROBLEM_ORSZAG_TANG = 0, /* mhd2d_glm_gpu.cu:443-451, unit periodic box        */
@@ -79,7 +83,7 @@ typedef struct {
   double hlld_tol;                  /* HLLD relative degeneracy tolerance      */
   double cfl;                       /* CFL number, 0 < cfl < 1                 */
   double alpha;                     /* GLM damping parameter, rate = c_h/alpha */
-  int order;                        /* pmhd_order (MUSCL + SSPRK2 or first)    */
+  int order;                        /* pmhd_order (MUSCL + SSPRK2, first, Hancock) */
   int solver;                       /* pmhd_solver_kind                        */
   int precision;                    /* pmhd_precision                          */
   int exact;                        /* 1: IEEE kernels without FMA contraction

@@ -422,6 +422,20 @@ PMHD_HD int glm_flux(const T* UL, const T* UR, T ch, bool use_hlld, T* F, const 
   return status;
 }
 
+// GLM-augmented physical flux along AX of a 9-slot conserved state: the
+// ideal-MHD flux (recovered with AX's summation order, i.e. the reference's
+// rotation for y), F[B_n] = psi, F[psi] = ch^2 B_n.  Used by the MUSCL-Hancock
+// predictor.
+template <class T, int AX>
+PMHD_HD void glm_phys_flux(const T* U, T ch, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  T W[NV8];
+  cons_to_prim<T, AX>(U, W, ph);
+  phys_flux<T, AX>(W, U[EN], F);
+  F[D::bn] = U[PSI];
+  F[PSI] = ch * ch * U[D::bn];
+}
+
 // ---- 9-slot helpers of the 2D driver (mhd2d_glm_cpu.cpp:90-161) ----------
 
 // Conserved -> primitive with psi carried in slot 8.

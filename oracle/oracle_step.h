@@ -231,6 +231,128 @@ int OF(or_run)(const or_config* cfg, OT* U, or_stats* st) {
   return rc;
 }
 
+/* ---- 2D MUSCL-Hancock variant (order "hancock") ----------------------------
+ * No 2D reference exists: this is the unsplit 2D extension of the reference's
+ * 1D Hancock predictor (mhd1d_cpu.cpp:203-235) on the 2D GLM solver's
+ * reconstruction, fluxes and update (mhd2d_glm_cpu.cpp:231-287): the four
+ * reconstructed faces of a cell advance by half a step with the cell's GLM
+ * flux differences in x and y (and half a step of psi damping), falling back
+ * to the unevolved face when the result is unusable; one interface flux per
+ * face from the evolved states; U += dt * rhs once per step. */
+
+/* Physical flux along dir of a 9-slot state with the GLM terms: the y flux
+ * is the x flux of the slot-swapped state (the reference's rotation). */
+static void OF(or_glm_phys_flux)(const OT U[9], OT ch, int dir, OT F[9], const OF(or_phys) * ph) {
+  OT a[8], W[8], f[8];
+  int k;
+  if (dir) OF(or_swap_xy)(U, a); else for (k = 0; k < 8; k++) a[k] = U[k];
+  OF(or_cons_to_prim)(a, W, ph);
+  OF(or_flux_x_w)(W, a[4], f);
+  f[5] = U[8];
+  if (dir) OF(or_swap_xy)(f, F); else for (k = 0; k < 8; k++) F[k] = f[k];
+  F[8] = ch * ch * a[5];
+}
+
+/* Half-step faces of one cell: Hx/Hy hold left/right (bottom/top) states. */
+static void OF(or_hancock_cell)(const OT* U, int c, int nxt, OT hx, OT hy, OT ch, OT hdamp, OT HXL[9], OT HXR[9],
+                                OT HYL[9], OT HYR[9], const OF(or_phys) * ph) {
+  OT P0[9], Pw[9], Pe[9], Ps[9], Pn[9], Pxl[9], Pxr[9], Pyl[9], Pyr[9];
+  OT F[4][9], corr[9];
+  OT* faces[4] = {HXL, HXR, HYL, HYR};
+  int k, f;
+  OF(or_state_to_prim9)(&U[c * 9], P0, ph);
+  OF(or_state_to_prim9)(&U[(c - 1) * 9], Pw, ph);
+  OF(or_state_to_prim9)(&U[(c + 1) * 9], Pe, ph);
+  OF(or_state_to_prim9)(&U[(c - nxt) * 9], Ps, ph);
+  OF(or_state_to_prim9)(&U[(c + nxt) * 9], Pn, ph);
+  OF(or_recon)(Pw, P0, Pe, Pxl, Pxr);
+  OF(or_recon)(Ps, P0, Pn, Pyl, Pyr);
+  OF(or_prim9_to_state)(Pxl, HXL, ph);
+  OF(or_prim9_to_state)(Pxr, HXR, ph);
+  OF(or_prim9_to_state)(Pyl, HYL, ph);
+  OF(or_prim9_to_state)(Pyr, HYR, ph);
+  for (f = 0; f < 4; f++) OF(or_glm_phys_flux)(faces[f], ch, f >= 2, F[f], ph);
+  for (k = 0; k < 9; k++) corr[k] = hx * (F[1][k] - F[0][k]) + hy * (F[3][k] - F[2][k]);
+  for (f = 0; f < 4; f++) {
+    OT h[9];
+    for (k = 0; k < 9; k++) h[k] = faces[f][k] - corr[k];
+    h[8] = h[8] - hdamp * faces[f][8];
+    if (OF(or_state_usable)(h, ph))
+      for (k = 0; k < 9; k++) faces[f][k] = h[k];
+  }
+}
+
+int OF(or_run_hancock)(const or_config* cfg, OT* U, or_stats* st) {
+  const int nx = cfg->nx, ny = cfg->ny, nxt = nx + 4, G = 2;
+  const size_t cells = (size_t)nxt * (ny + 4), n = cells * 9;
+  OF(or_phys) ph;
+  ph.gamma = (OT)cfg->gamma;
+  ph.tol = (OT)cfg->hlld_tol;
+  const OT dx = ((OT)cfg->x_max - (OT)cfg->x_min) / (OT)nx;
+  const OT dy = ((OT)cfg->y_max - (OT)cfg->y_min) / (OT)ny;
+  const OT cfl = (OT)cfg->cfl, alpha = (OT)cfg->alpha, t_end = (OT)cfg->t_end;
+  OT* H = (OT*)calloc(n * 4, sizeof(OT));
+  OT* Fx = (OT*)calloc(n, sizeof(OT));
+  OT* Gy = (OT*)calloc(n, sizeof(OT));
+  OT *HXL = H, *HXR = H + n, *HYL = H + 2 * n, *HYR = H + 3 * n;
+  int rc = 0, i, j, k;
+  OT t = (OT)st->t;
+  OF(or_apply_bc)(U, nx, ny, cfg->bc);
+  while (t < t_end && (cfg->max_steps < 0 || st->steps < cfg->max_steps)) {
+    OT ch = OF(or_max)(OF(or_max_speed)(U, nx, ny, &ph), (OT)1.0e-12);
+    st->ch_last = (double)ch;
+    OT max_rate = OF(or_max_rate)(U, nx, ny, dx, dy, ch, &ph);
+    if (max_rate <= (OT)0.0) { rc = 2; break; }
+    OT dt = cfl / max_rate;
+    if (t + dt > t_end) dt = t_end - t;
+    const OT damping = ch / OF(or_max)(alpha, (OT)1.0e-12);
+    const OT hx = (OT)0.5 * dt / dx, hy = (OT)0.5 * dt / dy, hdamp = (OT)0.5 * dt * damping;
+    for (j = G - 1; j < ny + G + 1; j++)
+      for (i = G - 1; i < nx + G + 1; i++) {
+        int c = j * nxt + i;
+        if ((j < G || j >= ny + G) && (i < G || i >= nx + G)) continue; /* corners: unused */
+        OF(or_hancock_cell)(U, c, nxt, hx, hy, ch, hdamp, &HXL[c * 9], &HXR[c * 9], &HYL[c * 9], &HYR[c * 9], &ph);
+      }
+    for (j = G; j < ny + G; j++)
+      for (i = G - 1; i < nx + G; i++) {
+        int c = j * nxt + i;
+        int s = OF(or_glm_flux)(&HXR[c * 9], &HXL[(c + 1) * 9], ch, cfg->use_hlld, 0, &Fx[c * 9], &ph);
+        if (cfg->use_hlld) {
+          st->x_evals++;
+          if (s == 1) st->degenerate++;
+          if (s == 2) st->nonphysical++;
+        }
+      }
+    for (j = G - 1; j < ny + G; j++)
+      for (i = G; i < nx + G; i++) {
+        int c = j * nxt + i;
+        int s = OF(or_glm_flux)(&HYR[c * 9], &HYL[(c + nxt) * 9], ch, cfg->use_hlld, 1, &Gy[c * 9], &ph);
+        if (cfg->use_hlld) {
+          st->y_evals++;
+          if (s == 1) st->degenerate++;
+          if (s == 2) st->nonphysical++;
+        }
+      }
+    for (j = G; j < ny + G; j++)
+      for (i = G; i < nx + G; i++) {
+        int id = j * nxt + i, im = id - 1, jm = id - nxt;
+        for (k = 0; k < 9; k++) {
+          OT rhs = -(Fx[id * 9 + k] - Fx[im * 9 + k]) / dx - (Gy[id * 9 + k] - Gy[jm * 9 + k]) / dy;
+          if (k == 8) rhs -= damping * U[id * 9 + 8];
+          U[id * 9 + k] = U[id * 9 + k] + dt * rhs;
+        }
+      }
+    OF(or_apply_bc)(U, nx, ny, cfg->bc);
+    if (!OF(or_all_usable)(U, nx, ny, &st->bad_i, &st->bad_j, &ph)) { rc = 3; break; }
+    t += dt;
+    st->steps++;
+  }
+  st->t = (double)t;
+  st->status = rc;
+  free(H); free(Fx); free(Gy);
+  return rc;
+}
+
 /* Exported per-point entry points (used to pin the restatement against the
  * reference's own headers through golden vectors). */
 void OF(or_point_cons_to_prim)(const OT U[8], OT W[8], double gamma) {

@@ -33,6 +33,10 @@ typedef struct {
 int or_run_f64(const or_config* cfg, double* U, or_stats* st);
 int or_run_f32(const or_config* cfg, float* U, or_stats* st);
 int or_run_mixed(const or_config* cfg, double* U, or_stats* st);
+/* The 2D MUSCL-Hancock variant (oracle_step.h): one predictor-corrector
+ * stage per step instead of SSPRK2; exit code 3 on an unusable cell. */
+int or_run_hancock_f64(const or_config* cfg, double* U, or_stats* st);
+int or_run_hancock_f32(const or_config* cfg, float* U, or_stats* st);
 
 void or_fill_ghosts_f64(const or_config* cfg, double* U);
 void or_fill_ghosts_f32(const or_config* cfg, float* U);

@@ -70,7 +70,7 @@ int main(int argc, char* argv[]) {
     std::cerr << "Error: problem must be 'ot' or 'kh'." << std::endl;
     return 1;
   }
-  if (order != "muscl" && order != "first") {
+  if (order != "muscl" && order != "first" && order != "hancock") {
     std::cerr << "Error: order must be 'muscl' or 'first'." << std::endl;
     return 1;
   }
@@ -86,7 +86,7 @@ int main(int argc, char* argv[]) {
   cfg.ny = ny;
   cfg.cfl = cfl;
   cfg.alpha = alpha;
-  cfg.order = order == "muscl" ? PMHD_ORDER_MUSCL : PMHD_ORDER_FIRST;
+  cfg.order = order == "muscl" ? PMHD_ORDER_MUSCL : (order == "hancock" ? PMHD_ORDER_HANCOCK : PMHD_ORDER_FIRST);
   cfg.solver = solver == "hlld" ? PMHD_SOLVER_HLLD : PMHD_SOLVER_HLL;
   cfg.precision = precision;
   if (const char* e = std::getenv("PMHD_EXACT")) cfg.exact = std::atoi(e) != 0;
@@ -112,7 +112,10 @@ int main(int argc, char* argv[]) {
   std::cout << "===== 2D ideal MHD Orszag-Tang vortex with mixed GLM (GPU) =====" << std::endl;
   std::cout << "Solver: " << (cfg.solver == PMHD_SOLVER_HLLD ? "HLLD" : "HLL") << std::endl;
   std::cout << "Reconstruction/time: "
-            << (cfg.order == PMHD_ORDER_MUSCL ? "MUSCL + SSPRK2" : "first-order + SSPRK2") << std::endl;
+            << (cfg.order == PMHD_ORDER_MUSCL ? "MUSCL + SSPRK2"
+                : cfg.order == PMHD_ORDER_HANCOCK ? "MUSCL-Hancock"
+                                                  : "first-order + SSPRK2")
+            << std::endl;
   std::cout << "Precision: " << (f32 ? 32 : 64) << " bit" << (f32 ? " (fp32)" : " (fp64)")
             << (precision == PMHD_MIXED ? " storage, fp32 flux (mixed)" : "") << std::endl;
   if (f32)

@@ -38,6 +38,7 @@ struct Ctrl {
   double last_ch, last_dt;      // ch and dt of the last step taken
   unsigned long long degenerate, nonphysical;  // HLLD fallbacks this advance
   unsigned long long active_stage_launches;    // stage launches that did work
+  double t_bad;                 // time at the start of the failing step (Hancock)
 };
 
 enum DeviceErr : int { DERR_NONE = 0, DERR_TMA_TIMEOUT = 1 };

@@ -1,0 +1,228 @@
+// hancock_kernel.cuh -- the 2D MUSCL-Hancock variant of the step
+// (pmhd_config.order = PMHD_ORDER_HANCOCK): one predictor-corrector stage per
+// step instead of the two SSPRK2 stages, so one pass over HBM per step.
+//
+// No 2D reference exists.  The scheme is the unsplit 2D extension of the
+// reference's 1D Hancock predictor (src/mhd/mhd1d_cpu.cpp:203-235) on the
+// 2D GLM solver's reconstruction, Riemann fluxes and update
+// (src/mhd/mhd2d_glm_cpu.cpp:231-287): a cell's four reconstructed faces
+// advance by half a step with its GLM flux differences in x and y and half a
+// step of psi damping (a face whose evolved state is unusable keeps its
+// unevolved state), one HLLD/HLL + GLM flux per interface from the evolved
+// states, U += dt * rhs.  The oracle's or_run_hancock is the same sequence.
+//
+// A CTA owns a 32 x TYH tile: it loads the 36 x (TYH+4) ghosted region
+// (plain coalesced loads; the SoA buffers keep ghost cells current), forms
+// primitives, the evolved faces of the (34 x (TYH+2)) box around the tile,
+// the tile's interface fluxes and the update, all staged in shared memory,
+// and stores the tile with its ghost copies into the other buffer (the step
+// of parity p reads buffer p, writes buffer p^1).  fp64 and fp32 policies.
+// Included by kernels.cu after stage_kernels.cuh.
+
+template <class T>
+struct HancockTile {
+  static constexpr int TYH = 8;
+  static constexpr int RW = TX + 4, RH = TYH + 4;  // region 36 x 12
+  static constexpr int NR = RW * RH;
+  static constexpr int BW = TX + 2, BH = TYH + 2;  // evolved-face box 34 x 10
+  static constexpr int NB = BW * BH;
+  static constexpr int NFX = (TX + 1) * TYH;       // x-interfaces of the tile
+  static constexpr int NGY = TX * (TYH + 1);       // y-interfaces
+  T U[NVAR][NR];
+  T P[NVAR][NR];                                   // primitives
+  T H[4][NVAR][NB];                                // evolved faces: x-left, x-right, y-bottom, y-top
+  T Fx[NVAR][NFX];                                 // interface fluxes
+  T Gy[NVAR][NGY];
+};
+
+// Prologue of a step: the stage-1 control update (zeroes the next step's
+// speed slot when the step runs, carries the slots forward when it does not).
+template <class Pol>
+__global__ void hancock_begin_kernel(const __grid_constant__ Member m, const int p) {
+  if (threadIdx.x != 0) return;
+  const StepVals<Pol> v = step_values<Pol, 1>(m, p);
+  member_bookkeeping<Pol, 1>(m, v, p);
+}
+
+template <class Pol, bool HLLD>
+__global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Member m, const int p) {
+  using T = typename Pol::S;
+  using HT = HancockTile<T>;
+  constexpr int RW = HT::RW, NR = HT::NR, BW = HT::BW, BH = HT::BH, NB = HT::NB, TYH = HT::TYH;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  HT& s = *reinterpret_cast<HT*>(smem_raw);
+  const Phys<T> ph = Phys<T>::make(m.gamma, m.tol);
+  const T* __restrict__ uin = static_cast<const T*>(p ? m.u1 : m.u);
+  T* __restrict__ uout = static_cast<T*>(p ? m.u : m.u1);
+  const int ntx = (m.nx + TX - 1) / TX;
+  const int i0 = (blockIdx.x % ntx) * TX, j0 = (blockIdx.x / ntx) * TYH;
+  const StepVals<Pol> v = step_values<Pol, 2>(m, p);
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (!v.active) {
+    // Carry the state (with its ghost copies) into the output buffer.
+    for (int q = tid; q < TX * TYH; q += blockDim.x) {
+      const int i = i0 + q % TX, j = j0 + q / TX;
+      if (i < m.nx && j < m.ny) {
+        T c[NVAR];
+#pragma unroll
+        for (int k = 0; k < NVAR; k++) c[k] = uin[(size_t)k * m.plane + (size_t)(j + GHOST) * m.pitch + (i + GHOST)];
+        store_cell<T>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, c);
+      }
+    }
+    if (blockIdx.x == 0 && tid == 0) member_bookkeeping<Pol, 2>(m, v, p);
+    return;
+  }
+  // Region: ghosted rows j0 .. j0+11, columns i0 .. i0+35 (clamped to the
+  // allocation; cells past the domain's ghost ring feed no in-domain update).
+  for (int q = tid; q < NR; q += blockDim.x) {
+    int gj = j0 + q / RW, gi = i0 + q % RW;
+    gj = gj < m.ny + 2 * GHOST ? gj : m.ny + 2 * GHOST - 1;
+    gi = gi < m.nx + 2 * GHOST ? gi : m.nx + 2 * GHOST - 1;
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) s.U[k][q] = uin[(size_t)k * m.plane + (size_t)gj * m.pitch + gi];
+  }
+  __syncthreads();
+  for (int q = tid; q < NR; q += blockDim.x) {
+    T U9[NVAR], P9[NVAR];
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) U9[k] = s.U[k][q];
+    state_to_prim9<T>(U9, P9, ph);
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) s.P[k][q] = P9[k];
+  }
+  __syncthreads();
+  const T dt = (T)v.dt, ch = (T)v.ch, dx = (T)m.dx, dy = (T)m.dy;
+  const T damping = ch / vmax((T)m.alpha, (T)1.0e-12);
+  const T hx = (T)0.5 * dt / dx, hy = (T)0.5 * dt / dy, hdamp = (T)0.5 * dt * damping;
+  // Evolved faces of the box cells (region rows 1..10, columns 1..34; the
+  // four box corners feed no interface of the tile).
+  for (int q = tid; q < NB; q += blockDim.x) {
+    const int br = q / BW, bc = q % BW;
+    if ((br == 0 || br == BH - 1) && (bc == 0 || bc == BW - 1)) continue;
+    const int c = (br + 1) * RW + (bc + 1);
+    T P0[NVAR], Pw[NVAR], Pe[NVAR], Ps[NVAR], Pn[NVAR], Pl[NVAR], Pr[NVAR];
+    T F[4][NVAR], Uf[4][NVAR];
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) {
+      P0[k] = s.P[k][c];
+      Pw[k] = s.P[k][c - 1];
+      Pe[k] = s.P[k][c + 1];
+      Ps[k] = s.P[k][c - RW];
+      Pn[k] = s.P[k][c + RW];
+    }
+    recon_cell<T>(Pw, P0, Pe, Pl, Pr);
+    prim9_to_state<T>(Pl, Uf[0], ph);
+    prim9_to_state<T>(Pr, Uf[1], ph);
+    recon_cell<T>(Ps, P0, Pn, Pl, Pr);
+    prim9_to_state<T>(Pl, Uf[2], ph);
+    prim9_to_state<T>(Pr, Uf[3], ph);
+    glm_phys_flux<T, 0>(Uf[0], ch, F[0], ph);
+    glm_phys_flux<T, 0>(Uf[1], ch, F[1], ph);
+    glm_phys_flux<T, 1>(Uf[2], ch, F[2], ph);
+    glm_phys_flux<T, 1>(Uf[3], ch, F[3], ph);
+    T corr[NVAR];
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) corr[k] = hx * (F[1][k] - F[0][k]) + hy * (F[3][k] - F[2][k]);
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      T h[NVAR];
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) h[k] = Uf[f][k] - corr[k];
+      h[PSI] = h[PSI] - hdamp * Uf[f][PSI];
+      const bool ok = state_usable<T>(h, ph);
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) s.H[f][k][q] = ok ? h[k] : Uf[f][k];
+    }
+  }
+  __syncthreads();
+  // Interface fluxes: x-interface (r, c) = between tile columns c-1 and c
+  // (c = 0..32) of tile row r; y-interface (r, c) = between tile rows r-1
+  // and r (r = 0..8) of tile column c.
+  T* Fx = &s.Fx[0][0];
+  T* Gy = &s.Gy[0][0];
+  unsigned n_deg = 0, n_np = 0;
+  for (int q = tid; q < HT::NFX + HT::NGY; q += blockDim.x) {
+    T a[NVAR], b[NVAR], F[NVAR];
+    int st;
+    if (q < HT::NFX) {
+      const int r = q / (TX + 1), c = q % (TX + 1);
+      const int bl = (r + 1) * BW + c, br = bl + 1;  // box cells left / right of the interface
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) {
+        a[k] = s.H[1][k][bl];
+        b[k] = s.H[0][k][br];
+      }
+      st = glm_flux<T, 0>(a, b, ch, HLLD, F, ph);
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) Fx[k * HT::NFX + q] = F[k];
+    } else {
+      const int g = q - HT::NFX, r = g / TX, c = g % TX;
+      const int bb = r * BW + (c + 1), bt = bb + BW;  // box cells below / above
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) {
+        a[k] = s.H[3][k][bb];
+        b[k] = s.H[2][k][bt];
+      }
+      st = glm_flux<T, 1>(a, b, ch, HLLD, F, ph);
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) Gy[k * HT::NGY + g] = F[k];
+    }
+    if (HLLD) {
+      // Count each interface of the domain once: interface I (between
+      // cells I-1 and I) by the tile with i0 <= I < i0 + 32, and I = nx by
+      // the last tile; likewise in y.
+      bool inside;
+      if (q < HT::NFX) {
+        const int r = q / (TX + 1), c = q % (TX + 1), I = i0 + c;
+        inside = j0 + r < m.ny && I <= m.nx && (c < TX || I == m.nx);
+      } else {
+        const int g = q - HT::NFX, r = g / TX, c = g % TX, J = j0 + r;
+        inside = i0 + c < m.nx && J <= m.ny && (r < TYH || J == m.ny);
+      }
+      if (inside) {
+        n_deg += st == HLLD_FALLBACK_DEGENERATE ? 1u : 0u;
+        n_np += st == HLLD_FALLBACK_NONPHYSICAL ? 1u : 0u;
+      }
+    }
+  }
+  __syncthreads();
+  // Update, store with ghost copies, usability and next-step speed.
+  const Phys<T> phR = ph;
+  unsigned long long sp = 0;
+  for (int q = tid; q < TX * TYH; q += blockDim.x) {
+    const int r = q / TX, c = q % TX;
+    const int i = i0 + c, j = j0 + r;
+    if (i >= m.nx || j >= m.ny) continue;
+    const int rc = (r + 2) * RW + (c + 2);
+    T Un[NVAR];
+#pragma unroll
+    for (int k = 0; k < NVAR; k++) {
+      T rhs = -(Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c]) / dx -
+              (Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c]) / dy;
+      if (k == PSI) rhs -= damping * s.U[PSI][rc];
+      Un[k] = s.U[k][rc] + dt * rhs;
+    }
+    store_cell<T>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, Un);
+    if (!state_usable<T>(Un, ph)) {
+      atomicMin(&m.ctrl->bad1, j * m.nx + i);
+      m.ctrl->bad_step = v.step;
+      m.ctrl->t_bad = (double)v.t;
+    } else {
+      T P9[NVAR];
+      state_to_prim9<T>(Un, P9, ph);
+      const unsigned long long b = speed_bits((double)cell_speed<T>(P9, phR));
+      sp = b > sp ? b : sp;
+    }
+  }
+  sp = warp_max_u64(sp);
+  if (HLLD) {
+    n_deg = warp_sum_u32(n_deg);
+    n_np = warp_sum_u32(n_np);
+  }
+  if (lane == 0) {
+    if (sp) atomicMax(&m.ctrl->chbits[p ^ 1], sp);
+    if (HLLD && n_deg) atomicAdd(&m.ctrl->degenerate, (unsigned long long)n_deg);
+    if (HLLD && n_np) atomicAdd(&m.ctrl->nonphysical, (unsigned long long)n_np);
+  }
+  if (blockIdx.x == 0 && tid == 0) member_bookkeeping<Pol, 2>(m, v, p);
+}

@@ -76,6 +76,10 @@ struct KernelTable {
                             void* aos, cudaStream_t s);
   // Shared memory per CTA of the stage kernel with tile height kTileHeights[ty_idx].
   size_t (*stage_smem)(int precision, int ty_idx);
+  // One MUSCL-Hancock step of a single grid: part 0 = the control prologue,
+  // part 1 = the step (reads m.u for parity 0 / m.u1 for parity 1, writes
+  // the other).  fp64 and fp32 only.
+  cudaError_t (*hancock)(int precision, int hlld, int part, const Member& m, int parity, cudaStream_t s);
 };
 
 const KernelTable& kernel_table_exact();

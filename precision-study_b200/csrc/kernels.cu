@@ -11,6 +11,8 @@
 namespace pmhd {
 namespace PMHD_KNS {
 
+#include "hancock_kernel.cuh"  // no includes of its own; lives in this namespace
+
 template <class Pol, int STAGE, bool HLLD, int TY, bool BATCHED>
 static cudaError_t set_smem_attr() {
   return cudaFuncSetAttribute(stage_kernel<Pol, STAGE, HLLD, TY, BATCHED>,
@@ -39,10 +41,20 @@ static cudaError_t init_pol() {
   return init_pol_ty<Pol, kTileHeights[1]>();
 }
 
+template <class Pol, bool HLLD>
+static cudaError_t init_hancock() {
+  return cudaFuncSetAttribute(hancock_kernel<Pol, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(HancockTile<typename Pol::S>));
+}
+
 static cudaError_t init() {
   cudaError_t e;
   if ((e = init_pol<PolF64>()) != cudaSuccess) return e;
   if ((e = init_pol<PolF32>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolF64, true>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolF64, false>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolF32, true>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolF32, false>()) != cudaSuccess) return e;
   return init_pol<PolMixed>();
 }
 
@@ -196,6 +208,30 @@ static cudaError_t launch_soa_to_aos(int precision, const void* u, long long pla
   return cudaGetLastError();
 }
 
+template <class Pol>
+static cudaError_t hancock_pol(int hlld, int part, const Member& m, int parity, cudaStream_t s) {
+  if (part == 0) {
+    hancock_begin_kernel<Pol><<<1, 32, 0, s>>>(m, parity);
+    return cudaGetLastError();
+  }
+  const unsigned grid = (unsigned)(((m.nx + TX - 1) / TX) * ((m.ny + HancockTile<double>::TYH - 1) /
+                                                            HancockTile<double>::TYH));
+  const size_t smem = sizeof(HancockTile<typename Pol::S>);
+  if (hlld)
+    hancock_kernel<Pol, true><<<grid, 256, smem, s>>>(m, parity);
+  else
+    hancock_kernel<Pol, false><<<grid, 256, smem, s>>>(m, parity);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_hancock(int precision, int hlld, int part, const Member& m, int parity, cudaStream_t s) {
+  switch (precision) {
+    case PREC_FP64: return hancock_pol<PolF64>(hlld, part, m, parity, s);
+    case PREC_FP32: return hancock_pol<PolF32>(hlld, part, m, parity, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
 }  // namespace PMHD_KNS
 
 #define PMHD_STR2(x) #x
@@ -207,7 +243,8 @@ const KernelTable& PMHD_TABLE_FN(PMHD_KNS)() {
   static const KernelTable t = {PMHD_STR(PMHD_KNS),          PMHD_KNS::init,
                                 PMHD_KNS::launch_stage,      PMHD_KNS::ctas_per_sm,
                                 PMHD_KNS::launch_speed,      PMHD_KNS::launch_aos_to_soa,
-                                PMHD_KNS::launch_soa_to_aos, PMHD_KNS::stage_smem};
+                                PMHD_KNS::launch_soa_to_aos, PMHD_KNS::stage_smem,
+                                PMHD_KNS::launch_hancock};
   return t;
 }
 

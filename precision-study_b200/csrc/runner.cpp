@@ -9,9 +9,14 @@ cudaError_t Runner::enqueue_steps(int nsteps) const {
     const int p = n & 1;
     cudaError_t e = pre_step ? pre_step(p) : cudaSuccess;
     if (e != cudaSuccess) return e;
-    e = kt->stage(precision, hlld, 1, choice.ty_idx, b, single, p, choice.grid, stream);
-    if (e != cudaSuccess) return e;
-    e = kt->stage(precision, hlld, 2, choice.ty_idx, b, single, p, choice.grid, stream);
+    if (hancock) {
+      if (!single) return cudaErrorNotSupported;
+      e = kt->hancock(precision, hlld, 0, *single, p, stream);
+      if (e == cudaSuccess) e = kt->hancock(precision, hlld, 1, *single, p, stream);
+    } else {
+      e = kt->stage(precision, hlld, 1, choice.ty_idx, b, single, p, choice.grid, stream);
+      if (e == cudaSuccess) e = kt->stage(precision, hlld, 2, choice.ty_idx, b, single, p, choice.grid, stream);
+    }
     if (e != cudaSuccess) return e;
     if (post_step) {
       e = post_step(p);

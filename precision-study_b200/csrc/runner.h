@@ -35,6 +35,7 @@ class Runner {
   Batch batch[kNumTileHeights];
   const Member* single = nullptr;  // host copy of a one-grid batch's member, or nullptr
   LaunchChoice choice;
+  int hancock = 0;  // MUSCL-Hancock steps (single grid) instead of SSPRK2 stages
   // Optional work enqueued before and after every step (argument: the
   // step's parity), captured into the graphs with the stage launches.
   std::function<cudaError_t(int)> pre_step, post_step;

@@ -118,9 +118,11 @@ int check_args(const pmhd_config* c) {
   if (!(c->alpha > 0.0)) return PMHD_ERR_ARG;
   if (!(c->gamma > 1.0)) return PMHD_ERR_ARG;
   if (!(c->hlld_tol >= 0.0)) return PMHD_ERR_ARG;
-  if (c->order != PMHD_ORDER_FIRST && c->order != PMHD_ORDER_MUSCL) return PMHD_ERR_ARG;
+  if (c->order != PMHD_ORDER_FIRST && c->order != PMHD_ORDER_MUSCL && c->order != PMHD_ORDER_HANCOCK)
+    return PMHD_ERR_ARG;
   if (c->solver != PMHD_SOLVER_HLL && c->solver != PMHD_SOLVER_HLLD) return PMHD_ERR_ARG;
   if (c->precision < PMHD_FP64 || c->precision > PMHD_MIXED) return PMHD_ERR_ARG;
+  if (c->order == PMHD_ORDER_HANCOCK && c->precision == PMHD_MIXED) return PMHD_ERR_UNSUPPORTED;
   for (int k = 0; k < 4; k++)
     if (c->bc[k] < PMHD_BC_PERIODIC || c->bc[k] > PMHD_BC_TRANSMISSIVE) return PMHD_ERR_ARG;
   if ((c->bc[0] == PMHD_BC_PERIODIC) != (c->bc[1] == PMHD_BC_PERIODIC)) return PMHD_ERR_ARG;
@@ -270,6 +272,7 @@ int pmhd_create(const pmhd_config* cfg, pmhd_solver** out) {
     s->run.kt = s->kt;
     s->run.precision = cfg->precision;
     s->run.hlld = cfg->solver == PMHD_SOLVER_HLLD ? 1 : 0;
+    s->run.hancock = cfg->order == PMHD_ORDER_HANCOCK ? 1 : 0;
     s->run.stream = s->stream;
     for (int t = 0; t < kNumTileHeights; t++) {
       Batch& b = s->run.batch[t];
@@ -394,7 +397,7 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
                        0, s->stream));
   const int big = s->cfg.steps_per_graph;
   long long tune_steps = 0;
-  if (s->cfg.autotune && !s->tuned && (max_steps < 0 || max_steps >= 32)) {
+  if (s->cfg.autotune && !s->run.hancock && !s->tuned && (max_steps < 0 || max_steps >= 32)) {
     // Live steps timed per kernel variant; identical results for every variant.
     const int per = 2;
     PMHD_CU(s->run.tune(per, &s->tune_result));
@@ -470,7 +473,9 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   const long long done_steps = h.step[0] - s->steps;
   const int hlld = s->cfg.solver == PMHD_SOLVER_HLLD;
-  long long stages = 2 * done_steps;
+  // Flux passes: two per SSPRK2 step, one per Hancock step.
+  const int per_step = s->run.hancock ? 1 : 2;
+  long long stages = per_step * done_steps;
   int status = PMHD_OK;
   if (h.err) {
     status = PMHD_ERR_TIMEOUT;
@@ -499,6 +504,13 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   }
   s->t = h.t[0];
   s->steps = h.step[0];
+  if (s->run.hancock && status == PMHD_ERR_STAGE1) {
+    // The failing Hancock step's launch already advanced the control slots;
+    // report the state the failure left, at the step and time it started
+    // (as the SSPRK2 path and the reference do).
+    s->t = h.t_bad;
+    s->steps = h.bad_step;
+  }
   s->stats.t = s->t;
   s->stats.steps = s->steps;
   s->stats.status = status;
@@ -547,7 +559,7 @@ static const char* precision_name(int p) { return p == PMHD_FP32 ? "fp32" : (p =
 int pmhd_dat_filename(const pmhd_solver* s, const char* prob_base, char* buf, size_t len) {
   if (!s || !prob_base || !buf || len == 0) return PMHD_ERR_ARG;
   const int n = std::snprintf(buf, len, "%s_glm_%s_%s_%s_N%dx%d.dat", prob_base,
-                              s->cfg.order == PMHD_ORDER_MUSCL ? "muscl" : "first",
+                              s->cfg.order == PMHD_ORDER_MUSCL ? "muscl" : (s->cfg.order == PMHD_ORDER_HANCOCK ? "hancock" : "first"),
                               s->cfg.solver == PMHD_SOLVER_HLLD ? "hlld" : "hll", precision_name(s->cfg.precision),
                               s->cfg.nx, s->cfg.ny);
   return (n < 0 || (size_t)n >= len) ? PMHD_ERR_ARG : PMHD_OK;
@@ -575,7 +587,8 @@ int pmhd_write_dat(pmhd_solver* s, const char* path, const char* title) {
       o << v;
     return o.str();
   };
-  const char* order = s->cfg.order == PMHD_ORDER_MUSCL ? "muscl" : "first";
+  const char* order =
+      s->cfg.order == PMHD_ORDER_MUSCL ? "muscl" : (s->cfg.order == PMHD_ORDER_HANCOCK ? "hancock" : "first");
   const char* solver = s->cfg.solver == PMHD_SOLVER_HLLD ? "hlld" : "hll";
   hd << "# " << (title ? title : "Orszag-Tang ideal MHD with mixed GLM (GPU)") << "\n";
   hd << "# nx " << s->cfg.nx << " ny " << s->cfg.ny << " t " << real(s->t) << " gamma " << real(s->cfg.gamma)

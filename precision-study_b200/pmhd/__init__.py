@@ -25,7 +25,7 @@ OK, ERR_ARG, ERR_RATE, ERR_STAGE1, ERR_STAGE2, ERR_IO, ERR_CUDA = 0, 1, 2, 3, 4,
 ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE = -1, -2, -3, -4
 FP64, FP32, MIXED = 0, 1, 2
 BC_PERIODIC, BC_REFLECT, BC_TRANSMISSIVE = 0, 1, 2
-ORDER_FIRST, ORDER_MUSCL = 0, 1
+ORDER_FIRST, ORDER_MUSCL, ORDER_HANCOCK = 0, 1, 2
 SOLVER_HLL, SOLVER_HLLD, SOLVER_HLLC = 0, 1, 2
 PROBLEM_ORSZAG_TANG, PROBLEM_KH_REF, PROBLEM_KH_REFLECT, PROBLEM_BRIO_WU_2D, PROBLEM_BRIO_WU_TORUS = 0, 1, 2, 3, 4
 LAYOUT_INTERIOR, LAYOUT_GHOSTED = 0, 1
@@ -226,7 +226,7 @@ def make_config(nx=128, ny=128, precision="fp64", exact=False, order="muscl", so
     c.nx, c.ny = nx, ny
     c.x_min, c.x_max, c.y_min, c.y_max = domain
     c.gamma, c.hlld_tol, c.cfl, c.alpha = gamma, hlld_tol, cfl, alpha
-    c.order = ORDER_MUSCL if order == "muscl" else ORDER_FIRST
+    c.order = {"muscl": ORDER_MUSCL, "first": ORDER_FIRST, "hancock": ORDER_HANCOCK}[order]
     c.solver = SOLVER_HLLD if solver == "hlld" else SOLVER_HLL
     c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     c.exact = int(bool(exact))

@@ -64,6 +64,9 @@ def lib():
             fn.argtypes = [P(OrConfig), ptr, P(OrStats)]
             fn.restype = ctypes.c_int
         for name, ptr in (("f64", dp), ("f32", fp)):
+            fn = getattr(_lib, "or_run_hancock_" + name)
+            fn.argtypes = [P(OrConfig), ptr, P(OrStats)]
+            fn.restype = ctypes.c_int
             fn = getattr(_lib, "or_init_ref_problem_" + name)
             fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 5 + [ptr]
             fn.restype = None
@@ -137,11 +140,12 @@ def init_ref_problem(prec, problem, nx, ny, domain=(0.0, 1.0, 0.0, 1.0), gamma=5
     return U
 
 
-def run(prec, cfg, U, t0=0.0, steps0=0):
-    """Advance the ghosted AoS state U in place.  prec: f64 | f32 | mixed."""
+def run(prec, cfg, U, t0=0.0, steps0=0, hancock=False):
+    """Advance the ghosted AoS state U in place.  prec: f64 | f32 | mixed
+    (SSPRK2), f64 | f32 with hancock=True (the MUSCL-Hancock variant)."""
     st = OrStats()
     st.t, st.steps = t0, steps0
-    fn = getattr(lib(), "or_run_" + prec)
+    fn = getattr(lib(), ("or_run_hancock_" if hancock else "or_run_") + prec)
     assert U.dtype == (np.float32 if prec == "f32" else np.float64)
     assert U.flags["C_CONTIGUOUS"] and U.shape == (cfg.ny + 4, cfg.nx + 4, 9)
     fn(ctypes.byref(cfg), _ptr(U), ctypes.byref(st))
