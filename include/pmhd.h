@@ -179,6 +179,16 @@ int pmhd_diagnostics(pmhd_solver* s, double out[3]);
  * the leading "# "; order/solver/precision names go into the second line. */
 int pmhd_write_dat(pmhd_solver* s, const char* path, const char* title);
 
+/* Restart files (no counterpart in the reference, which only writes .dat
+ * output): pmhd_write_restart stores the state (the GHOSTED layout, in the
+ * precision's element type), the time and the step count in a small binary
+ * file ("PMHDRST1", int32 nx, ny, precision, element bytes, double t, int64
+ * steps, values); pmhd_read_restart loads one into a handle of the same grid
+ * and precision (PMHD_ERR_ARG otherwise, PMHD_ERR_IO on a bad file).  A run
+ * resumed from a restart gives the same bits as one that never stopped. */
+int pmhd_write_restart(pmhd_solver* s, const char* path);
+int pmhd_read_restart(pmhd_solver* s, const char* path);
+
 /* Output file name the reference would use for this configuration:
  * {prob}_glm_{order}_{solver}_{fp64|fp32|mixed}_N{nx}x{ny}.dat */
 int pmhd_dat_filename(const pmhd_solver* s, const char* prob_base, char* buf, size_t len);

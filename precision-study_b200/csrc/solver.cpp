@@ -565,6 +565,53 @@ int pmhd_dat_filename(const pmhd_solver* s, const char* prob_base, char* buf, si
   return (n < 0 || (size_t)n >= len) ? PMHD_ERR_ARG : PMHD_OK;
 }
 
+int pmhd_write_restart(pmhd_solver* s, const char* path) {
+  if (!s || !path) return PMHD_ERR_ARG;
+  const size_t n = (size_t)(s->cfg.nx + 4) * (s->cfg.ny + 4) * 9;
+  std::vector<unsigned char> buf(n * s->elem);
+  const int rc = pmhd_get_state(s, buf.data(), PMHD_LAYOUT_GHOSTED);
+  if (rc != PMHD_OK) return rc;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return PMHD_ERR_IO;
+  const int hdr[4] = {s->cfg.nx, s->cfg.ny, s->cfg.precision, (int)s->elem};
+  const double t = s->t;
+  const long long steps = s->steps;
+  bool ok = std::fwrite("PMHDRST1", 1, 8, f) == 8 && std::fwrite(hdr, sizeof(int), 4, f) == 4 &&
+            std::fwrite(&t, sizeof(t), 1, f) == 1 && std::fwrite(&steps, sizeof(steps), 1, f) == 1 &&
+            std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? PMHD_OK : PMHD_ERR_IO;
+}
+
+int pmhd_read_restart(pmhd_solver* s, const char* path) {
+  if (!s || !path) return PMHD_ERR_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return PMHD_ERR_IO;
+  char magic[8];
+  int hdr[4];
+  double t = 0.0;
+  long long steps = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PMHDRST1", 8) == 0 &&
+            std::fread(hdr, sizeof(int), 4, f) == 4 && std::fread(&t, sizeof(t), 1, f) == 1 &&
+            std::fread(&steps, sizeof(steps), 1, f) == 1;
+  if (!ok) {
+    std::fclose(f);
+    return PMHD_ERR_IO;
+  }
+  if (hdr[0] != s->cfg.nx || hdr[1] != s->cfg.ny || hdr[2] != s->cfg.precision || hdr[3] != (int)s->elem) {
+    std::fclose(f);
+    return PMHD_ERR_ARG;
+  }
+  const size_t n = (size_t)(s->cfg.nx + 4) * (s->cfg.ny + 4) * 9;
+  std::vector<unsigned char> buf(n * s->elem);
+  ok = std::fread(buf.data(), 1, buf.size(), f) == buf.size();
+  std::fclose(f);
+  if (!ok) return PMHD_ERR_IO;
+  int rc = pmhd_set_state(s, buf.data(), PMHD_LAYOUT_GHOSTED);
+  if (rc == PMHD_OK) rc = pmhd_set_time(s, t, steps);
+  return rc;
+}
+
 int pmhd_write_dat(pmhd_solver* s, const char* path, const char* title) {
   if (!s || !path) return PMHD_ERR_ARG;
   const ProblemGrid g = grid_of(s);

@@ -46,7 +46,7 @@ EXPORTS = (
     "pmhd_learned_num_pairs", "pmhd_learned_train", "pmhd_learned_run", "pmhd_learned_fine_run",
     "pmhd_learned_save", "pmhd_learned_load",
     "pmhd_euler2d_create", "pmhd_euler2d_advance", "pmhd_euler2d_get_prim", "pmhd_euler2d_destroy",
-    "pmhd_euler1d_run",
+    "pmhd_euler1d_run", "pmhd_write_restart", "pmhd_read_restart",
 )
 
 
@@ -186,6 +186,8 @@ def load():
         "pmhd_euler2d_get_prim": ([vp, vp], i),
         "pmhd_euler2d_destroy": ([vp], i),
         "pmhd_euler1d_run": ([i, i, i, i, i, i, vp, P(EulerStats)], i),
+        "pmhd_write_restart": ([vp, ctypes.c_char_p], i),
+        "pmhd_read_restart": ([vp, ctypes.c_char_p], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -323,6 +325,12 @@ class Solver:
     def write_dat(self, path, title=None):
         _check(load().pmhd_write_dat(self._h, path.encode(), title.encode() if title else None),
                "pmhd_write_dat")
+
+    def write_restart(self, path):
+        _check(load().pmhd_write_restart(self._h, path.encode()), "pmhd_write_restart")
+
+    def read_restart(self, path):
+        _check(load().pmhd_read_restart(self._h, path.encode()), "pmhd_read_restart")
 
     def dat_filename(self, prob_base="orszag_tang"):
         buf = ctypes.create_string_buffer(512)

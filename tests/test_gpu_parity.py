@@ -176,3 +176,26 @@ def test_fma_mode_close_to_oracle(pmhd_lib, oracle, prec):
     assert sg.steps == so.steps
     rel = pmhd_lib.relative_l2(interior(Uo), interior(Ug))
     assert np.all(rel <= FMA_TOL[prec]), rel
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_restart_file_resumes_bit_for_bit(pmhd_lib, tmp_path, prec):
+    path = str(tmp_path / "ot.rst")
+    with pmhd_lib.Solver(nx=48, ny=40, precision=prec, exact=True) as a:
+        a.init_problem(0)
+        a.advance(t_end=0.08, max_steps=9)
+        a.write_restart(path)
+    with pmhd_lib.Solver(nx=48, ny=40, precision=prec, exact=True) as b:
+        b.read_restart(path)
+        st_b = b.advance(t_end=0.08)
+        Ub = b.get_state(layout=pmhd_lib.LAYOUT_GHOSTED)
+    with pmhd_lib.Solver(nx=48, ny=40, precision=prec, exact=True) as c:
+        c.init_problem(0)
+        st_c = c.advance(t_end=0.08)
+        Uc = c.get_state(layout=pmhd_lib.LAYOUT_GHOSTED)
+    assert st_b.steps == st_c.steps and st_b.t == st_c.t
+    np.testing.assert_array_equal(Ub, Uc)
+    with pmhd_lib.Solver(nx=40, ny=40, precision=prec) as d:
+        with pytest.raises(pmhd_lib.PmhdError) as e:
+            d.read_restart(path)
+        assert e.value.status == pmhd_lib.ERR_ARG
