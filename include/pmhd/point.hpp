@@ -228,10 +228,15 @@ PMHD_HD bool positive_state(const T* U, const Phys<T>& ph) {
 }
 
 // Star state behind an outer fast wave of speed s (mhdHlldStarStateX,
-// mhd_common.hpp:445-511).  bn is the (shared) normal field.
-template <class T, int AX>
-PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
-                      const Phys<T>& ph) {
+// mhd_common.hpp:445-511).  bn is the (shared) normal field.  vts receives
+// the star tangential velocities.
+//
+// FAST = true (the performance build only, never the parity build): the same
+// state with two reciprocals instead of six divisions, and the positivity
+// test from the star primitives already at hand instead of a conserved ->
+// primitive recovery (equal up to rounding).
+template <class T, int AX, bool FAST = false>
+PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us, T* vts, const Phys<T>& ph) {
   using D = Dir<AX>;
   const T rho = vmax(W[RHO], rho_floor<T>());
   const T vn = W[D::vn], vt1 = W[D::vt1], vt2 = W[D::vt2];
@@ -242,21 +247,40 @@ PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
   const T sms = s - sm;
   const T wave_scale = vmax(vabs(s), vabs(sm));
   if (hlld_small(sms, wave_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
-  const T rho_s = rho * smv / sms;
-  if (rho_s <= rho_floor<T>()) return HLLD_FALLBACK_NONPHYSICAL;
-  const T denom = rho * smv * sms - bn * bn;
-  const T denom_scale = vabs(rho * smv * sms) + bn * bn;
-  if (hlld_small(denom, denom_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
-  const T common = sm - vn;
-  const T vt1_s = vt1 - bn * bt1 * common / denom;
-  const T vt2_s = vt2 - bn * bt2 * common / denom;
-  const T bt1_s = bt1 * (rho * smv * smv - bn * bn) / denom;
-  const T bt2_s = bt2 * (rho * smv * smv - bn * bn) / denom;
+  T rho_s, vt1_s, vt2_s, bt1_s, bt2_s, e_s;
   const T b2 = bn * bn + bt1 * bt1 + bt2 * bt2;
   const T pt = p + (T)0.5 * b2;
   const T vdotb = vn * bn + vt1 * bt1 + vt2 * bt2;
-  const T vbs = sm * bn + vt1_s * bt1_s + vt2_s * bt2_s;
-  const T e_s = (smv * e - pt * vn + pt_star * sm + bn * (vdotb - vbs)) / sms;
+  if (FAST) {
+    const T inv_sms = (T)1.0 / sms;
+    rho_s = rho * smv * inv_sms;
+    if (rho_s <= rho_floor<T>()) return HLLD_FALLBACK_NONPHYSICAL;
+    const T denom = rho * smv * sms - bn * bn;
+    const T denom_scale = vabs(rho * smv * sms) + bn * bn;
+    if (hlld_small(denom, denom_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
+    const T inv_den = (T)1.0 / denom;
+    const T cb = bn * (sm - vn) * inv_den;
+    const T fb = (rho * smv * smv - bn * bn) * inv_den;
+    vt1_s = vt1 - bt1 * cb;
+    vt2_s = vt2 - bt2 * cb;
+    bt1_s = bt1 * fb;
+    bt2_s = bt2 * fb;
+    const T vbs = sm * bn + vt1_s * bt1_s + vt2_s * bt2_s;
+    e_s = (smv * e - pt * vn + pt_star * sm + bn * (vdotb - vbs)) * inv_sms;
+  } else {
+    rho_s = rho * smv / sms;
+    if (rho_s <= rho_floor<T>()) return HLLD_FALLBACK_NONPHYSICAL;
+    const T denom = rho * smv * sms - bn * bn;
+    const T denom_scale = vabs(rho * smv * sms) + bn * bn;
+    if (hlld_small(denom, denom_scale, ph)) return HLLD_FALLBACK_DEGENERATE;
+    const T common = sm - vn;
+    vt1_s = vt1 - bn * bt1 * common / denom;
+    vt2_s = vt2 - bn * bt2 * common / denom;
+    bt1_s = bt1 * (rho * smv * smv - bn * bn) / denom;
+    bt2_s = bt2 * (rho * smv * smv - bn * bn) / denom;
+    const T vbs = sm * bn + vt1_s * bt1_s + vt2_s * bt2_s;
+    e_s = (smv * e - pt * vn + pt_star * sm + bn * (vdotb - vbs)) / sms;
+  }
   Us[RHO] = rho_s;
   Us[D::vn] = rho_s * sm;
   Us[D::vt1] = rho_s * vt1_s;
@@ -265,6 +289,14 @@ PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
   Us[D::bn] = bn;
   Us[D::bt1] = bt1_s;
   Us[D::bt2] = bt2_s;
+  vts[0] = vt1_s;
+  vts[1] = vt2_s;
+  if (FAST) {
+    const T v2 = sm * sm + vt1_s * vt1_s + vt2_s * vt2_s;
+    const T b2s = bn * bn + bt1_s * bt1_s + bt2_s * bt2_s;
+    const T p_s = ph.gm1 * (e_s - (T)0.5 * rho_s * v2 - (T)0.5 * b2s);
+    return (p_s > p_floor<T>()) ? HLLD_OK : HLLD_FALLBACK_NONPHYSICAL;
+  }
   return positive_state<T, AX>(Us, ph) ? HLLD_OK : HLLD_FALLBACK_NONPHYSICAL;
 }
 
@@ -279,12 +311,13 @@ PMHD_HD int hlld_star(const T* U, const T* W, T s, T sm, T pt_star, T bn, T* Us,
 // front; the unused one never reaches F).  The side test `sm >= 0` selects
 // the same branch as the reference's chain sLs >= 0 / sm >= 0 / sRs >= 0
 // because sLs <= sm <= sRs, and NaN reaches the same last branch.
-template <class T, int AX>
-PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
+//
+// hlld_core takes the primitives of both sides as well; FAST as for
+// hlld_star (tangential star velocities reused, reciprocals, positivity of
+// the double-star states from their primitives).
+template <class T, int AX, bool FAST = false>
+PMHD_HD int hlld_core(const T* UL, const T* WL, const T* UR, const T* WR, T* F, const Phys<T>& ph) {
   using D = Dir<AX>;
-  T WL[NV8], WR[NV8];
-  cons_to_prim<T, AX>(UL, WL, ph);
-  cons_to_prim<T, AX>(UR, WR, ph);
   const T cfL = fast_speed<T, AX>(WL, ph);
   const T cfR = fast_speed<T, AX>(WR, ph);
   const T sL = vmin(WL[D::vn] - cfL, WR[D::vn] - cfR);
@@ -318,9 +351,9 @@ PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
     const T ptsL = ptL + rhoL * (sL - vnL) * (sm - vnL);
     const T ptsR = ptR + rhoR * (sR - vnR) * (sm - vnR);
     const T pts = (T)0.5 * (ptsL + ptsR);
-    T ULs[NV8], URs[NV8];
-    const int stL = hlld_star<T, AX>(UL, WL, sL, sm, pts, bn, ULs, ph);
-    const int stR = hlld_star<T, AX>(UR, WR, sR, sm, pts, bn, URs, ph);
+    T ULs[NV8], URs[NV8], vtL[2], vtR[2];
+    const int stL = hlld_star<T, AX, FAST>(UL, WL, sL, sm, pts, bn, ULs, vtL, ph);
+    const int stR = hlld_star<T, AX, FAST>(UR, WR, sR, sm, pts, bn, URs, vtR, ph);
     if (stL != HLLD_OK || stR != HLLD_OK) {
       status = (stL != HLLD_OK) ? stL : stR;
       break;
@@ -335,14 +368,23 @@ PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
       status = HLLD_FALLBACK_DEGENERATE;
       break;
     }
-    const T vt1Ls = ULs[D::vt1] / ULs[RHO], vt2Ls = ULs[D::vt2] / ULs[RHO];
+    const T vt1Ls = FAST ? vtL[0] : ULs[D::vt1] / ULs[RHO], vt2Ls = FAST ? vtL[1] : ULs[D::vt2] / ULs[RHO];
     const T bt1Ls = ULs[D::bt1], bt2Ls = ULs[D::bt2];
-    const T vt1Rs = URs[D::vt1] / URs[RHO], vt2Rs = URs[D::vt2] / URs[RHO];
+    const T vt1Rs = FAST ? vtR[0] : URs[D::vt1] / URs[RHO], vt2Rs = FAST ? vtR[1] : URs[D::vt2] / URs[RHO];
     const T bt1Rs = URs[D::bt1], bt2Rs = URs[D::bt2];
-    const T vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) / den;
-    const T vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) / den;
-    const T bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) / den;
-    const T bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) / den;
+    T vt1D, vt2D, bt1D, bt2D;
+    if (FAST) {
+      const T inv_den = (T)1.0 / den;
+      vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) * inv_den;
+      vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) * inv_den;
+      bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) * inv_den;
+      bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) * inv_den;
+    } else {
+      vt1D = (sqL * vt1Ls + sqR * vt1Rs + sgn * (bt1Rs - bt1Ls)) / den;
+      vt2D = (sqL * vt2Ls + sqR * vt2Rs + sgn * (bt2Rs - bt2Ls)) / den;
+      bt1D = (sqL * bt1Rs + sqR * bt1Ls + sgn * sqL * sqR * (vt1Rs - vt1Ls)) / den;
+      bt2D = (sqL * bt2Rs + sqR * bt2Ls + sgn * sqL * sqR * (vt2Rs - vt2Ls)) / den;
+    }
     const T vbD = sm * bn + vt1D * bt1D + vt2D * bt2D;
     const T vbLs = sm * bn + vt1Ls * bt1Ls + vt2Ls * bt2Ls;
     const T vbRs = sm * bn + vt1Rs * bt1Rs + vt2Rs * bt2Rs;
@@ -364,7 +406,17 @@ PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
     URD[D::bt2] = bt2D;
     ULD[EN] = ULs[EN] - sgn * sqL * (vbLs - vbD);
     URD[EN] = URs[EN] + sgn * sqR * (vbRs - vbD);
-    if (!positive_state<T, AX>(ULD, ph) || !positive_state<T, AX>(URD, ph)) {
+    bool positive;
+    if (FAST) {
+      const T v2D = sm * sm + vt1D * vt1D + vt2D * vt2D;
+      const T b2D = bn * bn + bt1D * bt1D + bt2D * bt2D;
+      const T pLD = ph.gm1 * (ULD[EN] - (T)0.5 * ULD[RHO] * v2D - (T)0.5 * b2D);
+      const T pRD = ph.gm1 * (URD[EN] - (T)0.5 * URD[RHO] * v2D - (T)0.5 * b2D);
+      positive = ULD[RHO] > rho_floor<T>() && URD[RHO] > rho_floor<T>() && pLD > p_floor<T>() && pRD > p_floor<T>();
+    } else {
+      positive = positive_state<T, AX>(ULD, ph) && positive_state<T, AX>(URD, ph);
+    }
+    if (!positive) {
       status = HLLD_FALLBACK_NONPHYSICAL;
       break;
     }
@@ -391,6 +443,14 @@ PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
   } while (false);
   hll_flux<T, AX>(UL, UR, F, ph);
   return status;
+}
+
+template <class T, int AX>
+PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
+  T WL[NV8], WR[NV8];
+  cons_to_prim<T, AX>(UL, WL, ph);
+  cons_to_prim<T, AX>(UR, WR, ph);
+  return hlld_core<T, AX, false>(UL, WL, UR, WR, F, ph);
 }
 
 // Mixed-GLM interface flux along AX (mhdGlmNormalState + mhdGlmFluxX/Y,
@@ -434,6 +494,45 @@ PMHD_HD void glm_phys_flux(const T* U, T ch, T* F, const Phys<T>& ph) {
   phys_flux<T, AX>(W, U[EN], F);
   F[D::bn] = U[PSI];
   F[PSI] = ch * ch * U[D::bn];
+}
+
+// glm_flux from the two face PRIMITIVES (9 slots, as reconstructed), for the
+// performance build: the conserved states are formed once, the primitives
+// the flux needs are the face primitives with B_n replaced by B_n* and the
+// pressure shifted by gm1 * (B_n^2 - B_n*^2) / 2 (what recovering them from
+// the modified conserved state gives, up to rounding), so the Riemann solver
+// recovers nothing.
+template <class T, int AX>
+PMHD_HD int glm_flux_prim(const T* PL, const T* PR, T ch, bool use_hlld, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T ch_safe = vmax(ch, (T)1.0e-12);
+  const T bnL = PL[D::bn], bnR = PR[D::bn], psiL = PL[PSI], psiR = PR[PSI];
+  const T bns = (T)0.5 * (bnL + bnR) - (T)0.5 * (psiR - psiL) / ch_safe;
+  const T psis = (T)0.5 * (psiL + psiR) - (T)0.5 * ch_safe * (bnR - bnL);
+  T UL[NV8], UR[NV8];
+  prim_to_cons<T>(PL, UL, ph);
+  prim_to_cons<T>(PR, UR, ph);
+  UL[D::bn] = bns;
+  UR[D::bn] = bns;
+  int status = HLLD_OK;
+  if (use_hlld) {
+    T WL[NV8], WR[NV8];
+#pragma unroll
+    for (int k = 0; k < NV8; k++) {
+      WL[k] = PL[k];
+      WR[k] = PR[k];
+    }
+    WL[D::bn] = bns;
+    WR[D::bn] = bns;
+    WL[EN] = PL[EN] + (T)0.5 * ph.gm1 * (bnL - bns) * (bnL + bns);
+    WR[EN] = PR[EN] + (T)0.5 * ph.gm1 * (bnR - bns) * (bnR + bns);
+    status = hlld_core<T, AX, true>(UL, WL, UR, WR, F, ph);
+  } else {
+    hll_flux<T, AX>(UL, UR, F, ph);
+  }
+  F[D::bn] = psis;
+  F[PSI] = ch * ch * bns;
+  return status;
 }
 
 // ---- 9-slot helpers of the 2D driver (mhd2d_glm_cpu.cpp:90-161) ----------

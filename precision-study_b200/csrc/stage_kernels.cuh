@@ -47,6 +47,13 @@
 #error "PMHD_KNS (kernel namespace: exact or fast) must be defined"
 #endif
 
+// PMHD_FAST_FLUX = 1 in the performance build (see Makefile): the MUSCL
+// faces go to the Riemann solver as primitives (glm_flux_prim).  0 in the
+// parity build.
+#ifndef PMHD_FAST_FLUX
+#define PMHD_FAST_FLUX 0
+#endif
+
 namespace pmhd {
 namespace PMHD_KNS {
 
@@ -254,6 +261,15 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
       P2[k] = q[3 * stride];
     }
     recon_cell<R>(Pm, P0, P1, Pl, Pr);
+    if (PMHD_FAST_FLUX) {
+      // Performance build: hand the face primitives to the solver directly
+      // (glm_flux_prim) instead of a primitive -> conserved -> primitive trip.
+      R Pa[NVAR];
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) Pa[k] = Pr[k];
+      recon_cell<R>(P0, P1, P2, Pl, Pr);
+      return glm_flux_prim<R, 0>(Pa, Pl, ch, HLLD, F, ph);
+    }
     prim9_to_state<R>(Pr, UL, ph);
     recon_cell<R>(P0, P1, P2, Pl, Pr);
     prim9_to_state<R>(Pl, UR, ph);
