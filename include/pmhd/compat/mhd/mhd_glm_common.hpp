@@ -114,7 +114,8 @@ __host__ __device__ inline bool mhdConservedHasPositivePressure(const Real U[8])
 }
 __host__ __device__ inline int mhdHlldStarStateX(const Real U[8], const Real W[8], Real s, Real sm,
                                                  Real pt_star, Real bx, Real Ustar[8]) {
-  return pmhd::hlld_star<Real, 0>(U, W, s, sm, pt_star, bx, Ustar, mhdCompatPhys());
+  Real vts[2];
+  return pmhd::hlld_star<Real, 0>(U, W, s, sm, pt_star, bx, Ustar, vts, mhdCompatPhys());
 }
 __host__ __device__ inline int mhdHlldFluxX(const Real UL[8], const Real UR[8], Real F[8]) {
   return pmhd::hlld_flux<Real, 0>(UL, UR, F, mhdCompatPhys());

@@ -445,19 +445,21 @@ PMHD_HD int hlld_core(const T* UL, const T* WL, const T* UR, const T* WR, T* F, 
   return status;
 }
 
-template <class T, int AX>
+template <class T, int AX, bool FAST = false>
 PMHD_HD int hlld_flux(const T* UL, const T* UR, T* F, const Phys<T>& ph) {
   T WL[NV8], WR[NV8];
   cons_to_prim<T, AX>(UL, WL, ph);
   cons_to_prim<T, AX>(UR, WR, ph);
-  return hlld_core<T, AX, false>(UL, WL, UR, WR, F, ph);
+  return hlld_core<T, AX, FAST>(UL, WL, UR, WR, F, ph);
 }
 
 // Mixed-GLM interface flux along AX (mhdGlmNormalState + mhdGlmFluxX/Y,
 // mhd_glm_common.hpp:55-126): upwind B_n* and psi* of the linear GLM
 // subsystem, HLLD (or HLL) on the 8 MHD slots with B_n = B_n* on both sides,
 // F[B_n] = psi*, F[psi] = ch^2 B_n*.
-template <class T, int AX>
+//
+// FAST selects the performance-build HLLD arithmetic (hlld_core).
+template <class T, int AX, bool FAST = false>
 PMHD_HD int glm_flux(const T* UL, const T* UR, T ch, bool use_hlld, T* F, const Phys<T>& ph) {
   using D = Dir<AX>;
   const T ch_safe = vmax(ch, (T)1.0e-12);
@@ -474,7 +476,7 @@ PMHD_HD int glm_flux(const T* UL, const T* UR, T ch, bool use_hlld, T* F, const 
   b[D::bn] = bns;
   int status = HLLD_OK;
   if (use_hlld)
-    status = hlld_flux<T, AX>(a, b, F, ph);
+    status = hlld_flux<T, AX, FAST>(a, b, F, ph);
   else
     hll_flux<T, AX>(a, b, F, ph);
   F[D::bn] = psis;

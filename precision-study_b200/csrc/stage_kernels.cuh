@@ -261,9 +261,10 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
       P2[k] = q[3 * stride];
     }
     recon_cell<R>(Pm, P0, P1, Pl, Pr);
-    if (PMHD_FAST_FLUX) {
+    if (PMHD_FAST_FLUX && !Pol::kMixed) {
       // Performance build: hand the face primitives to the solver directly
       // (glm_flux_prim) instead of a primitive -> conserved -> primitive trip.
+      // (Mixed keeps the trip: its 96-register budget would spill.)
       R Pa[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Pa[k] = Pr[k];
@@ -280,7 +281,7 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
       UR[k] = sP[off[k] + base + 2 * stride];
     }
   }
-  return glm_flux<R, 0>(UL, UR, ch, HLLD, F, ph);
+  return glm_flux<R, 0, PMHD_FAST_FLUX != 0>(UL, UR, ch, HLLD, F, ph);
 }
 
 // Per-member step values (uniform for all tiles of a member in one launch).
