@@ -261,10 +261,11 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
       P2[k] = q[3 * stride];
     }
     recon_cell<R>(Pm, P0, P1, Pl, Pr);
-    if (PMHD_FAST_FLUX && !Pol::kMixed) {
-      // Performance build: hand the face primitives to the solver directly
-      // (glm_flux_prim) instead of a primitive -> conserved -> primitive trip.
-      // (Mixed keeps the trip: its 96-register budget would spill.)
+    if (PMHD_FAST_FLUX && sizeof(R) == 8) {
+      // Performance build, fp64: hand the face primitives to the solver
+      // directly (glm_flux_prim) instead of a primitive -> conserved ->
+      // primitive trip.  (The fp32-flux policies keep the trip: their
+      // register budgets would spill.)
       R Pa[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Pa[k] = Pr[k];
