@@ -18,6 +18,8 @@ serial CPU solver (built from its sources into oracle/_ref/) on the host
 cores instead; only rank 0 runs it.
 """
 import argparse
+import contextlib
+import datetime
 import json
 import os
 import re
@@ -51,7 +53,7 @@ def dist_env():
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -59,13 +61,20 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.out = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __enter__(self):
         try:
             self.out = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.out, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
         time.sleep(0.3)
@@ -80,26 +89,39 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        """Median SM clock and the throttle reasons seen during the marked
+        region (samples taken while it ran; if it was shorter than the
+        sampling interval, the first sample after it began)."""
         if self.proc is None or self.out is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.out.seek(0)
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in self.out:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+        t0 = self.t0 if self.t0 is not None else float("-inf")
+        t1 = self.t1 if self.t1 is not None else float("inf")
+        inside = [r for r in rows if t0 <= r[0] <= t1]
+        if not inside:
+            inside = [r for r in rows if r[0] >= t0][:1]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in inside:
+            for n, v in zip(names, r[3]):
                 if v.lower() == "active":
                     reasons.add(n)
-        loaded = [v for v in sm if smax and v > 0.5 * smax] or sm
-        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        sm = [r[1] for r in inside]
+        smax = inside[0][2] if inside else None
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "samples_in_region": sum(1 for r in rows if t0 <= r[0] <= t1),
+                "region_s": (self.t1 - self.t0) if self.t0 is not None and self.t1 is not None else None,
+                "reasons": sorted(reasons)}
 
 
 def measured_peaks():
@@ -181,14 +203,17 @@ def time_precision(pmhd, precision, n, warmup, steps, device, sampler=None):
     """Device-timed throughput of `steps` steps after `warmup` steps."""
     s = pmhd.Solver(nx=n, ny=n, precision=precision, device=device)
     s.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
-    if warmup:
-        s.advance(max_steps=warmup)
-    before = s.stats().kernel_launches
-    if sampler is not None:
-        with sampler:
-            st = s.advance(max_steps=steps)
-    else:
+    # The sampler starts before the warm-up, so the timed steps follow the
+    # warm-up steps without an idle gap.
+    with (sampler if sampler is not None else contextlib.nullcontext()):
+        if warmup:
+            s.advance(max_steps=warmup)
+        before = s.stats().kernel_launches
+        if sampler is not None:
+            sampler.mark_start()
         st = s.advance(max_steps=steps)
+        if sampler is not None:
+            sampler.mark_end()
     launches = st.kernel_launches - before
     return s, st, launches
 
@@ -311,7 +336,7 @@ def main():
     ap.add_argument("--ref-instances", type=int, default=16, help="max concurrent reference processes")
     ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
     ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
-    ap.add_argument("--ensemble-seed", type=int, default=2024)
+    ap.add_argument("--ensemble-seed", type=int, default=20261203)
     ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
     ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
     ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")

@@ -47,9 +47,11 @@
 #error "PMHD_KNS (kernel namespace: exact or fast) must be defined"
 #endif
 
-// PMHD_FAST_FLUX = 1 in the performance build (see Makefile): the MUSCL
-// faces go to the Riemann solver as primitives (glm_flux_prim).  0 in the
-// parity build.
+// PMHD_FAST_FLUX = 1 in the performance build (see Makefile): the HLLD
+// performance arithmetic, the binary64 MUSCL faces go to the Riemann solver
+// as primitives (glm_flux_prim), and tiles whose cells are all usable skip
+// the face usability tests of the reconstruction (cell_usable_fast).  0 in
+// the parity build.
 #ifndef PMHD_FAST_FLUX
 #define PMHD_FAST_FLUX 0
 #endif
@@ -144,6 +146,23 @@ struct Smem {
   static constexpr size_t gy_off = fx_off + align128(sizeof(R) * NVAR * G::FXN);
   static constexpr size_t total = gy_off + align128(sizeof(R) * NVAR * G::GYN);
 };
+
+// Performance build: whether a recovered cell may take part in a limited
+// reconstruction (positive density and pressure, all nine values finite; a
+// sum is non-finite exactly when a term is, barring overflow, which only
+// makes the test stricter).  When every cell of a tile is usable, every
+// minmod-limited face is usable too -- a face lies between the cell value and
+// the midpoint towards a neighbour, so it stays above the floors (up to the
+// rounding of that one operation) and finite -- and the tile skips the face
+// tests of the reference (reconstructPrimitiveDev, mhd2d_glm_gpu.cu:81-95).
+// A tile with any unusable cell runs them.
+template <class R>
+__device__ __forceinline__ bool cell_usable_fast(const R* P) {
+  R sum = P[0];
+#pragma unroll
+  for (int k = 1; k < NVAR; k++) sum += P[k];
+  return P[RHO] > rho_floor<R>() && P[EN] > p_floor<R>() && vfinite(sum);
+}
 
 // Primitive recovery of one cell in the storage precision.  PolF64/PolF32
 // follow the reference (stateToPrimitiveDev, mhd2d_glm_gpu.cu:53-58: three
@@ -243,15 +262,18 @@ __device__ __forceinline__ void store_cell(S* u, long long plane, int pitch, int
 //   stride 1 (x) or HX (y)
 //   o1/o2  plane offsets of the normal / first tangential velocity slot
 //   o5/o6  plane offsets of the normal / first tangential field slot
+//   checks whether the reconstruction runs the reference's face usability
+//          tests (always in the parity build; in the performance build only
+//          in tiles with an unusable cell, see cell_usable_fast)
 template <class Pol, bool HLLD, int TC>
-__device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, int stride, int o1, int o2, int o5,
-                                         int o6, int muscl, typename Pol::R ch, const Phys<typename Pol::R>& ph,
-                                         typename Pol::R* F) {
+__device__ __forceinline__ int face_flux(const typename Pol::R* sP, bool checks, int base, int stride, int o1,
+                                         int o2, int o5, int o6, int muscl, typename Pol::R ch,
+                                         const Phys<typename Pol::R>& ph, typename Pol::R* F) {
   using R = typename Pol::R;
   const int off[NVAR] = {0, o1, o2, 3 * TC, 4 * TC, o5, o6, 7 * TC, 8 * TC};
   R UL[NVAR], UR[NVAR];
   if (muscl) {
-    R Pm[NVAR], P0[NVAR], P1[NVAR], P2[NVAR], Pl[NVAR], Pr[NVAR];
+    R Pm[NVAR], P0[NVAR], P1[NVAR], P2[NVAR], Pa[NVAR], Pb[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
       const R* q = sP + off[k] + base;
@@ -260,21 +282,27 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, int base, in
       P1[k] = q[2 * stride];
       P2[k] = q[3 * stride];
     }
-    recon_cell<R>(Pm, P0, P1, Pl, Pr);
-    if (PMHD_FAST_FLUX && sizeof(R) == 8) {
-      // Performance build, fp64: hand the face primitives to the solver
-      // directly (glm_flux_prim) instead of a primitive -> conserved ->
-      // primitive trip.  (The fp32-flux policies keep the trip: their
-      // register budgets would spill.)
-      R Pa[NVAR];
+    // Pa: right face of cell 0, Pb: left face of cell 1.
+    if (PMHD_FAST_FLUX && !checks) {
 #pragma unroll
-      for (int k = 0; k < NVAR; k++) Pa[k] = Pr[k];
-      recon_cell<R>(P0, P1, P2, Pl, Pr);
-      return glm_flux_prim<R, 0>(Pa, Pl, ch, HLLD, F, ph);
+      for (int k = 0; k < NVAR; k++) {
+        Pa[k] = P0[k] + (R)0.5 * minmod(P0[k] - Pm[k], P1[k] - P0[k]);
+        Pb[k] = P1[k] - (R)0.5 * minmod(P1[k] - P0[k], P2[k] - P1[k]);
+      }
+    } else {
+      R Pl[NVAR];
+      recon_cell<R>(Pm, P0, P1, Pl, Pa);
+      recon_cell<R>(P0, P1, P2, Pb, Pl);
     }
-    prim9_to_state<R>(Pr, UL, ph);
-    recon_cell<R>(P0, P1, P2, Pl, Pr);
-    prim9_to_state<R>(Pl, UR, ph);
+    if (PMHD_FAST_FLUX && sizeof(R) == 8) {
+      // Performance build, fp64: the face primitives go to the solver
+      // directly instead of a primitive -> conserved -> primitive trip.
+      // (The fp32-flux policies keep the trip: their register budgets would
+      // spill.)
+      return glm_flux_prim<R, 0>(Pa, Pb, ch, HLLD, F, ph);
+    }
+    prim9_to_state<R>(Pa, UL, ph);
+    prim9_to_state<R>(Pb, UR, ph);
   } else {  // first order: sP holds the conserved states
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
@@ -466,6 +494,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
 
     // ---- recovery, once per tile cell (halo corners are never used) -------
     // First order needs no primitives: the conserved states are staged.
+    bool usable = true;  // performance build: this thread's cells (cell_usable_fast)
     for (int q = tid; q < TC; q += NT) {
       const int cx = q % HX, cy = q / HX;
       if ((cx < 2 || cx >= TX + 2) && (cy < 2 || cy >= TY + 2)) continue;
@@ -478,10 +507,16 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
 #pragma unroll
         for (int k = 0; k < NVAR; k++) P9[k] = U9[k];
       }
+      R PR[NVAR];
 #pragma unroll
-      for (int k = 0; k < NVAR; k++) sP[k * TC + q] = (R)P9[k];
+      for (int k = 0; k < NVAR; k++) {
+        PR[k] = (R)P9[k];
+        sP[k * TC + q] = PR[k];
+      }
+      if (PMHD_FAST_FLUX && m.muscl) usable = usable && cell_usable_fast<R>(PR);
     }
-    __syncthreads();
+    const bool all_usable = __syncthreads_and(usable);
+    const bool checks = !PMHD_FAST_FLUX || !all_usable;
     // The next tile goes into the buffer no thread reads any more: this one
     // (just recovered) or, double-buffered, the previous tile's.
     const int next = next_active(tile + gridDim.x);
@@ -519,7 +554,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
       const int o1 = (axis ? 2 : 1) * TC, o2 = (axis ? 1 : 2) * TC;
       const int o5 = (axis ? 6 : 5) * TC, o6 = (axis ? 5 : 6) * TC;
       R F[NVAR];
-      const int st = face_flux<Pol, HLLD, TC>(sP, base, stride, o1, o2, o5, o6, m.muscl, v.ch, phR, F);
+      const int st = face_flux<Pol, HLLD, TC>(sP, checks, base, stride, o1, o2, o5, o6, m.muscl, v.ch, phR, F);
       R* out = axis ? sGy : sFx;
       const int n_out = axis ? GYN : FXN;
       const int item = axis ? fy * TX + fx : fy * (TX + 1) + fx;
