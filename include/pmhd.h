@@ -94,10 +94,10 @@ typedef struct {
   int steps_per_graph;              /* steps captured per CUDA graph, 0 = auto */
   int autotune;                     /* 1: the first pmhd_advance that runs at least
                                        32 steps times every stage-kernel variant
-                                       (32x8 / 32x4 tiles x resident CTAs per SM)
+                                       (32x16 / 32x8 tiles x resident CTAs per SM)
                                        on 2 live steps each and keeps the fastest;
                                        results do not depend on the variant.
-                                       0: 32x8 tiles, all resident CTAs.       */
+                                       0: 32x16 tiles, all resident CTAs.      */
 } pmhd_config;
 
 typedef struct {
@@ -115,7 +115,7 @@ typedef struct {
   unsigned long long kernel_launches; /* kernels that did work, total        */
   double device_ms;                 /* GPU time of the last pmhd_advance, from
                                        CUDA events on the handle's stream     */
-  int tile_height;                  /* stage-kernel tile height in use (8, 4)  */
+  int tile_height;                  /* stage-kernel tile height in use (16, 8) */
   int ctas;                         /* persistent CTAs per stage launch        */
   unsigned long long zone_cycles;   /* cells x steps of the last advance
                                        (summed over ensemble members)         */

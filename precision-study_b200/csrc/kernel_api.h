@@ -25,8 +25,8 @@ struct Ctrl;
 enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
 
 // Tile heights compiled into the library (tile width is 32).  Index into
-// Member::tm and the Batch tile tables.
-constexpr int kTileHeights[2] = {8, 4};
+// Member::tm and the Batch tile tables; index 0 is the default.
+constexpr int kTileHeights[2] = {16, 8};
 constexpr int kNumTileHeights = 2;
 
 // One grid of a batch; lives in device memory (64-byte aligned for the TMA

@@ -108,9 +108,12 @@ constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 //         (the update reads shared memory);
 //   minb  resident CTAs per SM the register allocation is sized for.
 // 32 x 8 tiles: fp64 1 buffer / 2 CTAs (a small spill beats halving the
-// resident warps), fp32 1 / 3, mixed 2 / 2.  32 x 4 tiles keep about the same
-// threads per SM.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64 override the
-// 32 x 8 values for tuning experiments.
+// resident warps), fp32 1 / 3, mixed 2 / 2.  32 x 16 tiles (the default: 17
+// warps, one CTA per SM) recompute fewer halo interfaces and recoveries
+// (2.09 interface solves and 1.41 recoveries per cell instead of 2.16 and
+// 1.63) and run 1-4 % faster at 4096^2; 32 x 4 tiles keep about the same
+// threads per SM as 32 x 8.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64
+// override the 32 x 8 values for tuning experiments.
 template <class Pol, int TY>
 struct Tune {
   static constexpr bool r64 = sizeof(typename Pol::R) == 8;

@@ -303,7 +303,7 @@ def test_default_ensemble_with_autotuner_matches_single_runs(pmhd_lib):
     common = dict(precision="mixed", exact=False)
     with pmhd_lib.Ensemble(ms, autotune=True, **common) as e:
         tot = e.advance()
-        assert tot.status == pmhd_lib.OK and tot.tile_height in (8, 4)
+        assert tot.status == pmhd_lib.OK and tot.tile_height in (16, 8)
         for k, d in enumerate(ms):
             U, st = _single(pmhd_lib, d, **common)
             assert abs(e.member_stats(k).steps - st.steps) <= 1
