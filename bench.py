@@ -461,19 +461,28 @@ def main():
     hancock = None
     if args.hancock > 0:
         hancock = {"grid": args.hancock, "workload": f"Orszag-Tang {args.hancock}^2, MUSCL-Hancock + HLLD + GLM",
-                   "algorithmic_bytes_per_zone_cycle": {"fp64": 144, "fp32": 72}}
-        for hp in ("fp64", "fp32"):
+                   "algorithmic_bytes_per_zone_cycle": {"fp64": 144, "mixed": 144, "fp32": 72}}
+        U64h = None
+        for hp in ("fp64", "mixed", "fp32"):
             sh = pmhd.Solver(nx=args.hancock, ny=args.hancock, precision=hp, order="hancock", device=local)
             sh.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
             sh.advance(max_steps=W + (W & 1))
             sth = sh.advance(max_steps=K + (K & 1))
-            sh.close()
             msh = max_over_ranks(sth.device_ms)
             nst = K + (K & 1)
-            bpc = 144 if hp == "fp64" else 72
+            bpc = hancock["algorithmic_bytes_per_zone_cycle"][hp]
             hancock[hp] = {"value": world * args.hancock ** 2 * nst / (msh / 1e3), "unit": UNIT,
                            "ms_per_step": msh / nst,
                            "achieved_GBs": bpc * args.hancock ** 2 * nst / (msh / 1e3) / 1e9}
+            if hp == "fp64":
+                U64h = sh.get_state()
+            elif hp == "mixed":
+                rel = pmhd.relative_l2(U64h, sh.get_state())
+                hancock["mixed"]["relL2_vs_fp64"] = {k: float(x) for k, x in
+                                                     zip(["rho", "mx", "my", "mz", "E", "Bx", "By", "Bz"], rel[:8])}
+                U64h = None
+            sh.close()
+        hancock["mixed_vs_fp64"] = hancock["mixed"]["value"] / hancock["fp64"]["value"]
 
     # ---- Euler sibling: fused split steps of the 2D Riemann problem ----------
     euler = None

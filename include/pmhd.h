@@ -63,8 +63,8 @@ typedef enum { PMHD_FP64 = 0, PMHD_FP32 = 1, PMHD_MIXED = 2 } pmhd_precision;
 typedef enum { PMHD_BC_PERIODIC = 0, PMHD_BC_REFLECT = 1, PMHD_BC_TRANSMISSIVE = 2 } pmhd_bc;
 /* PMHD_ORDER_HANCOCK: MUSCL reconstruction + Hancock half-step predictor, one
  * stage per step (no counterpart in the reference's 2D program; the 2D form
- * of its 1D predictor, src/mhd/mhd1d_cpu.cpp:203-235).  fp64 / fp32 only;
- * single grids only (not ensembles or pmhd_advance_noalloc). */
+ * of its 1D predictor, src/mhd/mhd1d_cpu.cpp:203-235).  All three precision
+ * policies; single grids only (not ensembles or pmhd_advance_noalloc). */
 typedef enum { PMHD_ORDER_FIRST = 0, PMHD_ORDER_MUSCL = 1, PMHD_ORDER_HANCOCK = 2 } pmhd_order;
 typedef enum { PMHD_SOLVER_HLL = 0, PMHD_SOLVER_HLLD = 1, PMHD_SOLVER_HLLC = 2 /* Euler */ } pmhd_solver_kind;
 typedef enum {

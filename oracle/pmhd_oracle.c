@@ -237,6 +237,111 @@ int or_run_mixed(const or_config* cfg, double* U, or_stats* st) {
   return rc;
 }
 
+/* Mixed-precision MUSCL-Hancock variant (this project's design; no
+ * reference counterpart): the binary64 recovery of every cell rounded to
+ * binary32, the binary32 faces, half-step predictor and GLM fluxes of the
+ * f32 Hancock restatement (oracle_step.h) from those primitives, and the
+ * binary64 update of the mixed SSPRK2 variant (binary32 flux differences,
+ * binary64 scaling, psi damping and accumulation), once per step. */
+static void or_mixed_hancock_cell(const float* P32, int c, int nxt, float hx, float hy, float ch, float hdamp,
+                                  float HXL[9], float HXR[9], float HYL[9], float HYR[9],
+                                  const or_phys_f32* ph) {
+  float Pxl[9], Pxr[9], Pyl[9], Pyr[9];
+  float F[4][9], corr[9];
+  float* faces[4] = {HXL, HXR, HYL, HYR};
+  int k, f;
+  or_recon_f32(&P32[(c - 1) * 9], &P32[c * 9], &P32[(c + 1) * 9], Pxl, Pxr);
+  or_recon_f32(&P32[(c - nxt) * 9], &P32[c * 9], &P32[(c + nxt) * 9], Pyl, Pyr);
+  or_prim9_to_state_f32(Pxl, HXL, ph);
+  or_prim9_to_state_f32(Pxr, HXR, ph);
+  or_prim9_to_state_f32(Pyl, HYL, ph);
+  or_prim9_to_state_f32(Pyr, HYR, ph);
+  for (f = 0; f < 4; f++) or_glm_phys_flux_f32(faces[f], ch, f >= 2, F[f], ph);
+  for (k = 0; k < 9; k++) corr[k] = hx * (F[1][k] - F[0][k]) + hy * (F[3][k] - F[2][k]);
+  for (f = 0; f < 4; f++) {
+    float h[9];
+    for (k = 0; k < 9; k++) h[k] = faces[f][k] - corr[k];
+    h[8] = h[8] - hdamp * faces[f][8];
+    if (or_state_usable_f32(h, ph))
+      for (k = 0; k < 9; k++) faces[f][k] = h[k];
+  }
+}
+
+int or_run_hancock_mixed(const or_config* cfg, double* U, or_stats* st) {
+  const int nx = cfg->nx, ny = cfg->ny, nxt = nx + 4, G = 2;
+  const size_t cells = (size_t)nxt * (ny + 4), n = cells * 9;
+  or_phys_f32 ph32;
+  const double gm1 = cfg->gamma - 1.0;
+  ph32.gamma = (float)cfg->gamma;
+  ph32.tol = (float)cfg->hlld_tol;
+  const double dx = (cfg->x_max - cfg->x_min) / (double)nx;
+  const double dy = (cfg->y_max - cfg->y_min) / (double)ny;
+  const double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy;
+  float* P32 = (float*)calloc(n, sizeof(float));
+  float* H = (float*)calloc(n * 4, sizeof(float));
+  float* Fx = (float*)calloc(n, sizeof(float));
+  float* Gy = (float*)calloc(n, sizeof(float));
+  float *HXL = H, *HXR = H + n, *HYL = H + 2 * n, *HYR = H + 3 * n;
+  int rc = 0, i, j, k;
+  double t = st->t;
+  or_apply_bc_f64(U, nx, ny, cfg->bc);
+  while (t < cfg->t_end && (cfg->max_steps < 0 || st->steps < cfg->max_steps)) {
+    or_mixed_recover(U, P32, cells, gm1);
+    const float ch = or_max_f32(or_mixed_max_speed(P32, nx, ny, &ph32), 1.0e-12f);
+    st->ch_last = (double)ch;
+    double dt = cfg->cfl / ((double)ch / dx + (double)ch / dy);
+    if (t + dt > cfg->t_end) dt = cfg->t_end - t;
+    const double damping = (double)ch / or_max_f64(cfg->alpha, 1.0e-12);
+    const float hx = (float)(0.5 * dt / dx), hy = (float)(0.5 * dt / dy), hdamp = (float)(0.5 * dt * damping);
+    for (j = G - 1; j < ny + G + 1; j++)
+      for (i = G - 1; i < nx + G + 1; i++) {
+        int c = j * nxt + i;
+        if ((j < G || j >= ny + G) && (i < G || i >= nx + G)) continue; /* corners: unused */
+        or_mixed_hancock_cell(P32, c, nxt, hx, hy, ch, hdamp, &HXL[c * 9], &HXR[c * 9], &HYL[c * 9], &HYR[c * 9],
+                              &ph32);
+      }
+    for (j = G; j < ny + G; j++)
+      for (i = G - 1; i < nx + G; i++) {
+        int c = j * nxt + i;
+        int s = or_glm_flux_f32(&HXR[c * 9], &HXL[(c + 1) * 9], ch, cfg->use_hlld, 0, &Fx[c * 9], &ph32);
+        if (cfg->use_hlld) {
+          st->x_evals++;
+          if (s == 1) st->degenerate++;
+          if (s == 2) st->nonphysical++;
+        }
+      }
+    for (j = G - 1; j < ny + G; j++)
+      for (i = G; i < nx + G; i++) {
+        int c = j * nxt + i;
+        int s = or_glm_flux_f32(&HYR[c * 9], &HYL[(c + nxt) * 9], ch, cfg->use_hlld, 1, &Gy[c * 9], &ph32);
+        if (cfg->use_hlld) {
+          st->y_evals++;
+          if (s == 1) st->degenerate++;
+          if (s == 2) st->nonphysical++;
+        }
+      }
+    for (j = G; j < ny + G; j++)
+      for (i = G; i < nx + G; i++) {
+        int id = j * nxt + i, im = id - 1, jm = id - nxt;
+        for (k = 0; k < 9; k++) {
+          float dfx = Fx[id * 9 + k] - Fx[im * 9 + k];
+          float dgy = Gy[id * 9 + k] - Gy[jm * 9 + k];
+          double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
+          if (k == 8) rhs -= damping * U[id * 9 + 8];
+          U[id * 9 + k] = U[id * 9 + k] + dt * rhs;
+        }
+      }
+    or_apply_bc_f64(U, nx, ny, cfg->bc);
+    if (!or_mixed_all_usable(U, nx, ny, &st->bad_i, &st->bad_j, gm1)) { rc = 3; break; }
+    t += dt;
+    st->steps++;
+  }
+  st->t = t;
+  st->status = rc;
+  free(P32); free(H); free(Fx); free(Gy);
+  return rc;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Initial conditions restated from mhd2d_glm_cpu.cpp:486-505 (Orszag-Tang)  */
 /* and mhd2d_glm_gpu.cu:421-441 (the reference's doubly periodic KH), in     */

@@ -37,6 +37,7 @@ int or_run_mixed(const or_config* cfg, double* U, or_stats* st);
  * stage per step instead of SSPRK2; exit code 3 on an unusable cell. */
 int or_run_hancock_f64(const or_config* cfg, double* U, or_stats* st);
 int or_run_hancock_f32(const or_config* cfg, float* U, or_stats* st);
+int or_run_hancock_mixed(const or_config* cfg, double* U, or_stats* st);
 
 void or_fill_ghosts_f64(const or_config* cfg, double* U);
 void or_fill_ghosts_f32(const or_config* cfg, float* U);

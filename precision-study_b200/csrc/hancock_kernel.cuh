@@ -16,10 +16,12 @@
 // primitives, the evolved faces of the (34 x (TYH+2)) box around the tile,
 // the tile's interface fluxes and the update, all staged in shared memory,
 // and stores the tile with its ghost copies into the other buffer (the step
-// of parity p reads buffer p, writes buffer p^1).  fp64 and fp32 policies.
+// of parity p reads buffer p, writes buffer p^1).  Policies as in the stage
+// kernel: fp64, fp32, and mixed (binary64 storage, recovery and update;
+// binary32 faces, predictor and fluxes).
 // Included by kernels.cu after stage_kernels.cuh.
 
-template <class T>
+template <class S, class R>
 struct HancockTile {
   static constexpr int TYH = 8;
   static constexpr int RW = TX + 4, RH = TYH + 4;  // region 36 x 12
@@ -28,12 +30,14 @@ struct HancockTile {
   static constexpr int NB = BW * BH;
   static constexpr int NFX = (TX + 1) * TYH;       // x-interfaces of the tile
   static constexpr int NGY = TX * (TYH + 1);       // y-interfaces
-  T U[NVAR][NR];
-  T P[NVAR][NR];                                   // primitives
-  T H[4][NVAR][NB];                                // evolved faces: x-left, x-right, y-bottom, y-top
-  T Fx[NVAR][NFX];                                 // interface fluxes
-  T Gy[NVAR][NGY];
+  S U[NVAR][NR];
+  R P[NVAR][NR];                                   // primitives
+  R H[4][NVAR][NB];                                // evolved faces: x-left, x-right, y-bottom, y-top
+  R Fx[NVAR][NFX];                                 // interface fluxes
+  R Gy[NVAR][NGY];
 };
+template <class Pol>
+using HancockTileOf = HancockTile<typename Pol::S, typename Pol::R>;
 
 // Prologue of a step: the stage-1 control update (zeroes the next step's
 // speed slot when the step runs, carries the slots forward when it does not).
@@ -46,14 +50,17 @@ __global__ void hancock_begin_kernel(const __grid_constant__ Member m, const int
 
 template <class Pol, bool HLLD>
 __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Member m, const int p) {
-  using T = typename Pol::S;
-  using HT = HancockTile<T>;
+  using S = typename Pol::S;   // storage, recovery, update
+  using R = typename Pol::R;   // faces, predictor, fluxes
+  using TT = typename Pol::TT;
+  using HT = HancockTileOf<Pol>;
   constexpr int RW = HT::RW, NR = HT::NR, BW = HT::BW, BH = HT::BH, NB = HT::NB, TYH = HT::TYH;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   HT& s = *reinterpret_cast<HT*>(smem_raw);
-  const Phys<T> ph = Phys<T>::make(m.gamma, m.tol);
-  const T* __restrict__ uin = static_cast<const T*>(p ? m.u1 : m.u);
-  T* __restrict__ uout = static_cast<T*>(p ? m.u : m.u1);
+  const Phys<S> phS = Phys<S>::make(m.gamma, m.tol);
+  const Phys<R> ph = Phys<R>::make(m.gamma, m.tol);
+  const S* __restrict__ uin = static_cast<const S*>(p ? m.u1 : m.u);
+  S* __restrict__ uout = static_cast<S*>(p ? m.u : m.u1);
   const int ntx = (m.nx + TX - 1) / TX;
   const int i0 = (blockIdx.x % ntx) * TX, j0 = (blockIdx.x / ntx) * TYH;
   const StepVals<Pol> v = step_values<Pol, 2>(m, p);
@@ -63,10 +70,10 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
     for (int q = tid; q < TX * TYH; q += blockDim.x) {
       const int i = i0 + q % TX, j = j0 + q / TX;
       if (i < m.nx && j < m.ny) {
-        T c[NVAR];
+        S c[NVAR];
 #pragma unroll
         for (int k = 0; k < NVAR; k++) c[k] = uin[(size_t)k * m.plane + (size_t)(j + GHOST) * m.pitch + (i + GHOST)];
-        store_cell<T>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, c);
+        store_cell<S>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, c);
       }
     }
     if (blockIdx.x == 0 && tid == 0) member_bookkeeping<Pol, 2>(m, v, p);
@@ -82,26 +89,30 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
     for (int k = 0; k < NVAR; k++) s.U[k][q] = uin[(size_t)k * m.plane + (size_t)gj * m.pitch + gi];
   }
   __syncthreads();
+  // Primitives in the storage precision (the mixed policy's binary64
+  // recovery), kept in the face precision.
   for (int q = tid; q < NR; q += blockDim.x) {
-    T U9[NVAR], P9[NVAR];
+    S U9[NVAR], P9[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) U9[k] = s.U[k][q];
-    state_to_prim9<T>(U9, P9, ph);
+    recover_cell<Pol>(U9, P9, phS);
 #pragma unroll
-    for (int k = 0; k < NVAR; k++) s.P[k][q] = P9[k];
+    for (int k = 0; k < NVAR; k++) s.P[k][q] = (R)P9[k];
   }
   __syncthreads();
-  const T dt = (T)v.dt, ch = (T)v.ch, dx = (T)m.dx, dy = (T)m.dy;
-  const T damping = ch / vmax((T)m.alpha, (T)1.0e-12);
-  const T hx = (T)0.5 * dt / dx, hy = (T)0.5 * dt / dy, hdamp = (T)0.5 * dt * damping;
+  // Step scalars in the time type; the predictor's in the face precision.
+  const TT dt = v.dt, dx = (TT)m.dx, dy = (TT)m.dy;
+  const R ch = v.ch;
+  const TT damping = (TT)ch / vmax((TT)m.alpha, (TT)1.0e-12);
+  const R hx = (R)((TT)0.5 * dt / dx), hy = (R)((TT)0.5 * dt / dy), hdamp = (R)((TT)0.5 * dt * damping);
   // Evolved faces of the box cells (region rows 1..10, columns 1..34; the
   // four box corners feed no interface of the tile).
   for (int q = tid; q < NB; q += blockDim.x) {
     const int br = q / BW, bc = q % BW;
     if ((br == 0 || br == BH - 1) && (bc == 0 || bc == BW - 1)) continue;
     const int c = (br + 1) * RW + (bc + 1);
-    T P0[NVAR], Pw[NVAR], Pe[NVAR], Ps[NVAR], Pn[NVAR], Pl[NVAR], Pr[NVAR];
-    T F[4][NVAR], Uf[4][NVAR];
+    R P0[NVAR], Pw[NVAR], Pe[NVAR], Ps[NVAR], Pn[NVAR], Pl[NVAR], Pr[NVAR];
+    R F[4][NVAR], Uf[4][NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
       P0[k] = s.P[k][c];
@@ -110,26 +121,26 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
       Ps[k] = s.P[k][c - RW];
       Pn[k] = s.P[k][c + RW];
     }
-    recon_cell<T>(Pw, P0, Pe, Pl, Pr);
-    prim9_to_state<T>(Pl, Uf[0], ph);
-    prim9_to_state<T>(Pr, Uf[1], ph);
-    recon_cell<T>(Ps, P0, Pn, Pl, Pr);
-    prim9_to_state<T>(Pl, Uf[2], ph);
-    prim9_to_state<T>(Pr, Uf[3], ph);
-    glm_phys_flux<T, 0>(Uf[0], ch, F[0], ph);
-    glm_phys_flux<T, 0>(Uf[1], ch, F[1], ph);
-    glm_phys_flux<T, 1>(Uf[2], ch, F[2], ph);
-    glm_phys_flux<T, 1>(Uf[3], ch, F[3], ph);
-    T corr[NVAR];
+    recon_cell<R>(Pw, P0, Pe, Pl, Pr);
+    prim9_to_state<R>(Pl, Uf[0], ph);
+    prim9_to_state<R>(Pr, Uf[1], ph);
+    recon_cell<R>(Ps, P0, Pn, Pl, Pr);
+    prim9_to_state<R>(Pl, Uf[2], ph);
+    prim9_to_state<R>(Pr, Uf[3], ph);
+    glm_phys_flux<R, 0>(Uf[0], ch, F[0], ph);
+    glm_phys_flux<R, 0>(Uf[1], ch, F[1], ph);
+    glm_phys_flux<R, 1>(Uf[2], ch, F[2], ph);
+    glm_phys_flux<R, 1>(Uf[3], ch, F[3], ph);
+    R corr[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) corr[k] = hx * (F[1][k] - F[0][k]) + hy * (F[3][k] - F[2][k]);
 #pragma unroll
     for (int f = 0; f < 4; f++) {
-      T h[NVAR];
+      R h[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) h[k] = Uf[f][k] - corr[k];
       h[PSI] = h[PSI] - hdamp * Uf[f][PSI];
-      const bool ok = state_usable<T>(h, ph);
+      const bool ok = state_usable<R>(h, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) s.H[f][k][q] = ok ? h[k] : Uf[f][k];
     }
@@ -138,11 +149,11 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
   // Interface fluxes: x-interface (r, c) = between tile columns c-1 and c
   // (c = 0..32) of tile row r; y-interface (r, c) = between tile rows r-1
   // and r (r = 0..8) of tile column c.
-  T* Fx = &s.Fx[0][0];
-  T* Gy = &s.Gy[0][0];
+  R* Fx = &s.Fx[0][0];
+  R* Gy = &s.Gy[0][0];
   unsigned n_deg = 0, n_np = 0;
   for (int q = tid; q < HT::NFX + HT::NGY; q += blockDim.x) {
-    T a[NVAR], b[NVAR], F[NVAR];
+    R a[NVAR], b[NVAR], F[NVAR];
     int st;
     if (q < HT::NFX) {
       const int r = q / (TX + 1), c = q % (TX + 1);
@@ -152,7 +163,7 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
         a[k] = s.H[1][k][bl];
         b[k] = s.H[0][k][br];
       }
-      st = glm_flux<T, 0>(a, b, ch, HLLD, F, ph);
+      st = glm_flux<R, 0>(a, b, ch, HLLD, F, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Fx[k * HT::NFX + q] = F[k];
     } else {
@@ -163,7 +174,7 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
         a[k] = s.H[3][k][bb];
         b[k] = s.H[2][k][bt];
       }
-      st = glm_flux<T, 1>(a, b, ch, HLLD, F, ph);
+      st = glm_flux<R, 1>(a, b, ch, HLLD, F, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Gy[k * HT::NGY + g] = F[k];
     }
@@ -187,30 +198,48 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
   }
   __syncthreads();
   // Update, store with ghost copies, usability and next-step speed.
-  const Phys<T> phR = ph;
   unsigned long long sp = 0;
   for (int q = tid; q < TX * TYH; q += blockDim.x) {
     const int r = q / TX, c = q % TX;
     const int i = i0 + c, j = j0 + r;
     if (i >= m.nx || j >= m.ny) continue;
     const int rc = (r + 2) * RW + (c + 2);
-    T Un[NVAR];
+    S Un[NVAR];
+    if constexpr (!Pol::kMixed) {
 #pragma unroll
-    for (int k = 0; k < NVAR; k++) {
-      T rhs = -(Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c]) / dx -
-              (Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c]) / dy;
-      if (k == PSI) rhs -= damping * s.U[PSI][rc];
-      Un[k] = s.U[k][rc] + dt * rhs;
+      for (int k = 0; k < NVAR; k++) {
+        R rhs = -(Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c]) / dx -
+                (Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c]) / dy;
+        if (k == PSI) rhs -= damping * s.U[PSI][rc];
+        Un[k] = s.U[k][rc] + dt * rhs;
+      }
+    } else {
+      // Binary32 flux differences, binary64 scaling and accumulation (as
+      // the mixed stage kernel).
+      const double inv_dx = 1.0 / m.dx, inv_dy = 1.0 / m.dy;
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) {
+        const float dfx = Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c];
+        const float dgy = Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c];
+        double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
+        if (k == PSI) rhs -= damping * s.U[PSI][rc];
+        Un[k] = s.U[k][rc] + dt * rhs;
+      }
     }
-    store_cell<T>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, Un);
-    if (!state_usable<T>(Un, ph)) {
+    store_cell<S>(uout, m.plane, m.pitch, i, j, m.nx, m.ny, m.bc, Un);
+    // stateIsUsable with the policy's recovery, which also gives the next
+    // step's signal speed.
+    S P9[NVAR];
+    recover_cell<Pol>(Un, P9, phS);
+    if (!(Un[RHO] > rho_floor<S>()) || !prim9_usable<S>(P9)) {
       atomicMin(&m.ctrl->bad1, j * m.nx + i);
       m.ctrl->bad_step = v.step;
       m.ctrl->t_bad = (double)v.t;
     } else {
-      T P9[NVAR];
-      state_to_prim9<T>(Un, P9, ph);
-      const unsigned long long b = speed_bits((double)cell_speed<T>(P9, phR));
+      R Pr[NVAR];
+#pragma unroll
+      for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
+      const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, ph));
       sp = b > sp ? b : sp;
     }
   }

@@ -44,7 +44,7 @@ static cudaError_t init_pol() {
 template <class Pol, bool HLLD>
 static cudaError_t init_hancock() {
   return cudaFuncSetAttribute(hancock_kernel<Pol, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(HancockTile<typename Pol::S>));
+                              (int)sizeof(HancockTileOf<Pol>));
 }
 
 static cudaError_t init() {
@@ -55,6 +55,8 @@ static cudaError_t init() {
   if ((e = init_hancock<PolF64, false>()) != cudaSuccess) return e;
   if ((e = init_hancock<PolF32, true>()) != cudaSuccess) return e;
   if ((e = init_hancock<PolF32, false>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolMixed, true>()) != cudaSuccess) return e;
+  if ((e = init_hancock<PolMixed, false>()) != cudaSuccess) return e;
   return init_pol<PolMixed>();
 }
 
@@ -214,9 +216,9 @@ static cudaError_t hancock_pol(int hlld, int part, const Member& m, int parity, 
     hancock_begin_kernel<Pol><<<1, 32, 0, s>>>(m, parity);
     return cudaGetLastError();
   }
-  const unsigned grid = (unsigned)(((m.nx + TX - 1) / TX) * ((m.ny + HancockTile<double>::TYH - 1) /
-                                                            HancockTile<double>::TYH));
-  const size_t smem = sizeof(HancockTile<typename Pol::S>);
+  constexpr int TYH = HancockTileOf<Pol>::TYH;
+  const unsigned grid = (unsigned)(((m.nx + TX - 1) / TX) * ((m.ny + TYH - 1) / TYH));
+  const size_t smem = sizeof(HancockTileOf<Pol>);
   if (hlld)
     hancock_kernel<Pol, true><<<grid, 256, smem, s>>>(m, parity);
   else
@@ -228,6 +230,7 @@ static cudaError_t launch_hancock(int precision, int hlld, int part, const Membe
   switch (precision) {
     case PREC_FP64: return hancock_pol<PolF64>(hlld, part, m, parity, s);
     case PREC_FP32: return hancock_pol<PolF32>(hlld, part, m, parity, s);
+    case PREC_MIXED: return hancock_pol<PolMixed>(hlld, part, m, parity, s);
     default: return cudaErrorNotSupported;
   }
 }

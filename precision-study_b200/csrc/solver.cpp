@@ -122,7 +122,6 @@ int check_args(const pmhd_config* c) {
     return PMHD_ERR_ARG;
   if (c->solver != PMHD_SOLVER_HLL && c->solver != PMHD_SOLVER_HLLD) return PMHD_ERR_ARG;
   if (c->precision < PMHD_FP64 || c->precision > PMHD_MIXED) return PMHD_ERR_ARG;
-  if (c->order == PMHD_ORDER_HANCOCK && c->precision == PMHD_MIXED) return PMHD_ERR_UNSUPPORTED;
   for (int k = 0; k < 4; k++)
     if (c->bc[k] < PMHD_BC_PERIODIC || c->bc[k] > PMHD_BC_TRANSMISSIVE) return PMHD_ERR_ARG;
   if ((c->bc[0] == PMHD_BC_PERIODIC) != (c->bc[1] == PMHD_BC_PERIODIC)) return PMHD_ERR_ARG;

@@ -63,6 +63,9 @@ def lib():
             fn = getattr(_lib, "or_run_" + name)
             fn.argtypes = [P(OrConfig), ptr, P(OrStats)]
             fn.restype = ctypes.c_int
+        fn = _lib.or_run_hancock_mixed
+        fn.argtypes = [P(OrConfig), dp, P(OrStats)]
+        fn.restype = ctypes.c_int
         for name, ptr in (("f64", dp), ("f32", fp)):
             fn = getattr(_lib, "or_run_hancock_" + name)
             fn.argtypes = [P(OrConfig), ptr, P(OrStats)]
@@ -141,8 +144,8 @@ def init_ref_problem(prec, problem, nx, ny, domain=(0.0, 1.0, 0.0, 1.0), gamma=5
 
 
 def run(prec, cfg, U, t0=0.0, steps0=0, hancock=False):
-    """Advance the ghosted AoS state U in place.  prec: f64 | f32 | mixed
-    (SSPRK2), f64 | f32 with hancock=True (the MUSCL-Hancock variant)."""
+    """Advance the ghosted AoS state U in place.  prec: f64 | f32 | mixed,
+    SSPRK2 or (hancock=True) the MUSCL-Hancock variant."""
     st = OrStats()
     st.t, st.steps = t0, steps0
     fn = getattr(lib(), ("or_run_hancock_" if hancock else "or_run_") + prec)

@@ -1,9 +1,11 @@
 """The 2D MUSCL-Hancock variant (order "hancock"): one predictor-corrector
 stage per step.  No 2D reference exists, so the oracle (or_run_hancock,
-oracle/oracle_step.h) is the unsplit 2D form of the reference's 1D Hancock
+oracle/oracle_step.h; the mixed policy's or_run_hancock_mixed,
+oracle/pmhd_oracle.c) is the unsplit 2D form of the reference's 1D Hancock
 predictor on the 2D solver's own pinned building blocks; parity is GPU vs
 that oracle (bit for bit in the exact build).  CPU tests check the oracle's
-conservation and its agreement with the SSPRK2 scheme at second order.
+conservation, its agreement with the SSPRK2 scheme at second order, and the
+mixed policy against binary64.
 """
 import numpy as np
 import pytest
@@ -54,17 +56,27 @@ def test_oracle_hancock_converges_at_second_order(oracle):
     assert errs[0] / errs[1] > 3.0, errs
 
 
-def test_hancock_mixed_precision_is_unsupported(pmhd_lib):
-    import ctypes
-    c = pmhd_lib.make_config(nx=16, ny=16, precision="mixed", order="hancock")
-    h = ctypes.c_void_p()
-    assert pmhd_lib.load().pmhd_create(ctypes.byref(c), ctypes.byref(h)) == pmhd_lib.ERR_UNSUPPORTED
+def test_oracle_hancock_mixed_tracks_fp64(oracle):
+    """Mixed policy (binary32 faces, predictor and fluxes; binary64 recovery
+    and update) against binary64 on a smooth Orszag-Tang run: conserved totals
+    kept to binary64 round-off, per-variable relative L2 at binary32 level."""
+    nx = ny = 64
+    U0 = oracle.init_ref_problem("f64", 0, nx, ny)
+    Um, sm = _oracle_hancock(oracle, "mixed", nx, ny, 0.1)
+    Ud, sd = _oracle_hancock(oracle, "fp64", nx, ny, 0.1)
+    assert sm.status == sd.status == 0 and sm.steps == sd.steps > 0
+    for k in (0, 1, 2, 4, 5, 6):
+        assert abs(interior(Um)[..., k].sum() - interior(U0)[..., k].sum()) < 1e-10 * max(1.0, np.abs(U0[..., k]).sum())
+    rel = np.sqrt(np.mean((interior(Um) - interior(Ud)) ** 2, axis=(0, 1))) / \
+        np.sqrt(np.mean(interior(Ud) ** 2, axis=(0, 1)) + 1e-300)
+    assert np.all(rel[[0, 1, 2, 4, 5, 6]] < 1e-5), rel
+    assert np.all(rel[[0, 1, 2, 4, 5, 6]] > 0.0), rel  # the binary32 stages are really used
 
 
 # ---- GPU ---------------------------------------------------------------------
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
 @pytest.mark.parametrize("solver", ["hlld", "hll"])
 def test_hancock_exact_bitwise_vs_oracle_ot(pmhd_lib, oracle, prec, solver):
     nx, ny, t_end = 40, 24, 0.06
@@ -78,7 +90,7 @@ def test_hancock_exact_bitwise_vs_oracle_ot(pmhd_lib, oracle, prec, solver):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "mixed"])
 def test_hancock_exact_bitwise_walls_and_partial_tiles(pmhd_lib, oracle, prec):
     """KH with reflecting y walls on a 50 x 36 grid (partial tiles in x and
     y), and the rotated Brio-Wu tube with transmissive walls."""
@@ -115,7 +127,7 @@ def test_hancock_step_limited_runs_resume_exactly(pmhd_lib, oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5), ("mixed", 1e-5)])
 def test_hancock_fast_build_close_to_the_oracle(pmhd_lib, oracle, prec, tol):
     nx = ny = 96
     Ug, sg = gpu_run(pmhd_lib, prec, nx, ny, 0.05, exact=False, order="hancock")
