@@ -319,6 +319,12 @@ int pmhd_learned_destroy(pmhd_learned* L);
  * steps, until the store is full.  *added (may be NULL) = pairs stored. */
 int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
                           int* added);
+/* As pmhd_learned_generate, but the coarse run keeps its own state after the
+ * first step (the restricted fine state is loaded once): pairs along the
+ * plain coarse trajectory, the states a corrected run meets, each with the
+ * restricted fine state at the same time as its target. */
+int pmhd_learned_generate_rollout(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
+                                  int every, int* added);
 int pmhd_learned_num_pairs(const pmhd_learned* L);
 
 /* `iters` Adam steps (cosine decay from lr) on minibatches of `batch` pairs

@@ -250,8 +250,15 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
 
 int pmhd_learned_num_pairs(const pmhd_learned* L) { return L ? L->npairs : 0; }
 
-int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
-                          int* added) {
+namespace {
+
+// Training pairs (before, plain coarse step, restricted fine state at the
+// same time) along a fine run.  rollout = false: every coarse step starts
+// from the restricted fine state; true: the coarse run keeps its own state
+// after the first step (the states a corrected run actually meets), and the
+// target stays the restricted fine state.
+int generate_pairs(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
+                   int* added, bool rollout) {
   if (added) *added = 0;
   if (!L || every < 1 || !(t_end > 0.0)) return PMHD_ERR_ARG;
   L_CU(cudaSetDevice(L->cfg.device));
@@ -280,7 +287,11 @@ int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, in
   cudaError_t e = restrict_state(vf.u, vf.pitch, vf.plane, vf.nx, vf.ny, r, cur, vf.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(vf.stream);
   while (e == cudaSuccess && rc == PMHD_OK && t < t_end && L->npairs < L->cfg.max_pairs) {
-    e = load_periodic(cur, vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, vc.stream);
+    if (!rollout || k == 0) {
+      e = load_periodic(cur, vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, vc.stream);
+    } else {
+      e = store_interior(vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, cur, vc.stream);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(vc.stream);
     if (e != cudaSuccess) break;
     pmhd_set_time(c.s, t, 0);
@@ -320,6 +331,18 @@ int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, in
     return PMHD_ERR_CUDA;
   }
   return rc;
+}
+
+}  // namespace
+
+int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
+                          int* added) {
+  return generate_pairs(L, problem, params, nparams, t_end, every, added, false);
+}
+
+int pmhd_learned_generate_rollout(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
+                                  int every, int* added) {
+  return generate_pairs(L, problem, params, nparams, t_end, every, added, true);
 }
 
 int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* losses) {

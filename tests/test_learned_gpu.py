@@ -246,3 +246,19 @@ def test_learned_correction_trains_and_beats_the_plain_coarse_grid(pmhd_lib, tmp
             corr2, sc2 = L2.run(OT, [1.0], t_end=t_end, use_net=True)
             assert sc2.steps == sc.steps
             np.testing.assert_allclose(corr2, corr, rtol=0, atol=1e-12 * np.abs(corr).max())
+
+
+def test_rollout_pairs_follow_the_coarse_trajectory(pmhd_lib):
+    """pmhd_learned_generate_rollout stores one pair per coarse step, as
+    pmhd_learned_generate does (the coarse run keeps its own state instead of
+    restarting from the restricted fine one, so its CFL steps and hence the
+    pair count may differ slightly), and a network trains on them."""
+    OT = pmhd_lib.PROBLEM_ORSZAG_TANG
+    counts = []
+    for rollout in (False, True):
+        with pmhd_lib.Learned(nx=32, ny=32, refine=2, max_pairs=200, seed=5) as L:
+            counts.append(L.generate(OT, [1.0], t_end=0.1, every=1, rollout=rollout))
+            if rollout:
+                losses = L.train(iters=200, batch=4, lr=2e-3)
+                assert np.all(np.isfinite(losses)) and losses[-20:].mean() < losses[:5].mean()
+    assert counts[0] > 10 and abs(counts[0] - counts[1]) <= 2
