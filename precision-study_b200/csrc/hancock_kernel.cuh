@@ -21,20 +21,31 @@
 // binary32 faces, predictor and fluxes).
 // Included by kernels.cu after stage_kernels.cuh.
 
+// Tile of one CTA.  The primitives are dead once the evolved faces exist,
+// so the interface fluxes reuse their storage.  Binary64 faces use 32 x 4
+// tiles: with 32 x 8 the tile needs ~200 KB and one CTA of 8 warps per SM
+// (latency-bound); at 32 x 4 two CTAs fit (98 KB; binary32 faces: 98 KB or
+// 82 KB at 32 x 8).  Registers are sized for two CTAs (128 per thread).
 template <class S, class R>
 struct HancockTile {
-  static constexpr int TYH = 8;
-  static constexpr int RW = TX + 4, RH = TYH + 4;  // region 36 x 12
+  static constexpr int TYH = sizeof(R) == 8 ? 4 : 8;
+  static constexpr int MINB = 2;                   // resident CTAs the registers are sized for
+  static constexpr int RW = TX + 4, RH = TYH + 4;  // region 36 x (TYH + 4)
   static constexpr int NR = RW * RH;
-  static constexpr int BW = TX + 2, BH = TYH + 2;  // evolved-face box 34 x 10
+  static constexpr int BW = TX + 2, BH = TYH + 2;  // evolved-face box 34 x (TYH + 2)
   static constexpr int NB = BW * BH;
   static constexpr int NFX = (TX + 1) * TYH;       // x-interfaces of the tile
   static constexpr int NGY = TX * (TYH + 1);       // y-interfaces
+  struct Fluxes {
+    R Fx[NVAR][NFX];                               // interface fluxes
+    R Gy[NVAR][NGY];
+  };
   S U[NVAR][NR];
-  R P[NVAR][NR];                                   // primitives
+  union {
+    R P[NVAR][NR];                                 // primitives
+    Fluxes f;                                      // after the evolved faces
+  };
   R H[4][NVAR][NB];                                // evolved faces: x-left, x-right, y-bottom, y-top
-  R Fx[NVAR][NFX];                                 // interface fluxes
-  R Gy[NVAR][NGY];
 };
 template <class Pol>
 using HancockTileOf = HancockTile<typename Pol::S, typename Pol::R>;
@@ -49,7 +60,7 @@ __global__ void hancock_begin_kernel(const __grid_constant__ Member m, const int
 }
 
 template <class Pol, bool HLLD>
-__global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Member m, const int p) {
+__global__ void __launch_bounds__(256, HancockTileOf<Pol>::MINB) hancock_kernel(const __grid_constant__ Member m, const int p) {
   using S = typename Pol::S;   // storage, recovery, update
   using R = typename Pol::R;   // faces, predictor, fluxes
   using TT = typename Pol::TT;
@@ -79,7 +90,7 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
     if (blockIdx.x == 0 && tid == 0) member_bookkeeping<Pol, 2>(m, v, p);
     return;
   }
-  // Region: ghosted rows j0 .. j0+11, columns i0 .. i0+35 (clamped to the
+  // Region: ghosted rows j0 .. j0+TYH+3, columns i0 .. i0+35 (clamped to the
   // allocation; cells past the domain's ghost ring feed no in-domain update).
   for (int q = tid; q < NR; q += blockDim.x) {
     int gj = j0 + q / RW, gi = i0 + q % RW;
@@ -105,7 +116,7 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
   const R ch = v.ch;
   const TT damping = (TT)ch / vmax((TT)m.alpha, (TT)1.0e-12);
   const R hx = (R)((TT)0.5 * dt / dx), hy = (R)((TT)0.5 * dt / dy), hdamp = (R)((TT)0.5 * dt * damping);
-  // Evolved faces of the box cells (region rows 1..10, columns 1..34; the
+  // Evolved faces of the box cells (region rows 1..TYH+2, columns 1..34; the
   // four box corners feed no interface of the tile).
   for (int q = tid; q < NB; q += blockDim.x) {
     const int br = q / BW, bc = q % BW;
@@ -148,9 +159,9 @@ __global__ void __launch_bounds__(256) hancock_kernel(const __grid_constant__ Me
   __syncthreads();
   // Interface fluxes: x-interface (r, c) = between tile columns c-1 and c
   // (c = 0..32) of tile row r; y-interface (r, c) = between tile rows r-1
-  // and r (r = 0..8) of tile column c.
-  R* Fx = &s.Fx[0][0];
-  R* Gy = &s.Gy[0][0];
+  // and r (r = 0..TYH) of tile column c.
+  R* Fx = &s.f.Fx[0][0];
+  R* Gy = &s.f.Gy[0][0];
   unsigned n_deg = 0, n_np = 0;
   for (int q = tid; q < HT::NFX + HT::NGY; q += blockDim.x) {
     R a[NVAR], b[NVAR], F[NVAR];
