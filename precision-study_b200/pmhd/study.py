@@ -6,12 +6,13 @@
         analysis/mhd/compare_precision.py (relL2 = RMS(a - b) / RMS(a)).
 
     python -m pmhd.study run --n 1024 --t-end 0.5 [--problem ot|kh_reflect]
+                             [--runs fp64,fp64_exact,fp32,mixed]
         Runs the same problem in fp64 (FMA), fp64 (exact IEEE, no FMA),
-        fp32 and mixed on one GPU and prints one JSON object: zone-cycles/s
-        of each, and the relative L2 of every other run against fp64 per
-        conserved variable and per .dat primitive column.  The exact-vs-FMA
-        fp64 pair is the rounding noise floor the mixed result is judged
-        against.
+        fp32 and mixed on one GPU (or the listed subset; fp64 always runs)
+        and prints one JSON object: zone-cycles/s of each, and the relative L2
+        of every other run against fp64 per conserved variable and per .dat
+        primitive column.  The exact-vs-FMA fp64 pair is the rounding noise
+        floor the mixed result is judged against.
 """
 import argparse
 import json
@@ -67,7 +68,11 @@ def run_case(n, ny, t_end, precision, exact, problem, domain, bc, params):
     return U, st, wall
 
 
-def run_study(n, t_end, problem_name, ny=None):
+ALL_RUNS = (("fp64", "fp64", False), ("fp64_exact", "fp64", True), ("fp32", "fp32", False),
+            ("mixed", "mixed", False))
+
+
+def run_study(n, t_end, problem_name, ny=None, runs_wanted=None):
     if problem_name == "kh_reflect":
         problem, domain, bc, params = PROBLEM_KH_REFLECT, (0.0, 1.0, -1.0, 1.0), (0, 0, 1, 1), [0.05, 0.1]
         ny = ny or 2 * n
@@ -76,8 +81,9 @@ def run_study(n, t_end, problem_name, ny=None):
         ny = ny or n
     runs = {}
     states = {}
-    for tag, prec, exact in (("fp64", "fp64", False), ("fp64_exact", "fp64", True), ("fp32", "fp32", False),
-                             ("mixed", "mixed", False)):
+    for tag, prec, exact in ALL_RUNS:
+        if runs_wanted is not None and tag != "fp64" and tag not in runs_wanted:
+            continue
         U, st, wall = run_case(n, ny, t_end, prec, exact, problem, domain, bc, params)
         states[tag] = U
         runs[tag] = {"steps": st.steps, "t": st.t, "device_s": st.device_ms / 1e3, "wall_s": wall,
@@ -85,7 +91,7 @@ def run_study(n, t_end, problem_name, ny=None):
                      "hlld_fallbacks": st.degenerate + st.nonphysical}
     ref = states["fp64"]
     prims_ref = conserved_to_dat_columns(ref)
-    for tag in ("fp64_exact", "fp32", "mixed"):
+    for tag in [t for t in ("fp64_exact", "fp32", "mixed") if t in states]:
         runs[tag]["relL2_conserved_vs_fp64"] = dict(zip(CONS_NAMES, map(float, relative_l2(ref, states[tag]))))
         runs[tag]["relL2_dat_vs_fp64"] = dict(zip(DAT_NAMES, map(float, relative_l2(
             prims_ref, conserved_to_dat_columns(states[tag])))))
@@ -103,11 +109,13 @@ def main(argv=None):
     r.add_argument("--ny", type=int, default=None)
     r.add_argument("--t-end", type=float, default=0.5)
     r.add_argument("--problem", choices=["ot", "kh_reflect"], default="ot")
+    r.add_argument("--runs", default=None, help="comma list of fp64_exact, fp32, mixed (fp64 always runs)")
     args = ap.parse_args(argv)
     if args.cmd == "compare":
         compare_dat(args.a, args.b)
     else:
-        print(json.dumps(run_study(args.n, args.t_end, args.problem, args.ny)))
+        wanted = None if args.runs is None else set(args.runs.split(","))
+        print(json.dumps(run_study(args.n, args.t_end, args.problem, args.ny, wanted)))
     return 0
 
 
