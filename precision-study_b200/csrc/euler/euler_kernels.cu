@@ -118,23 +118,10 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
   __syncthreads();
 }
 
-template <class T, int TY>
-__device__ __forceinline__ void prims(Tile<T, TY>& s, int r0, int r1, int c0, int c1) {
-  const int w = c1 - c0, n = (r1 - r0) * w;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    const int id = (r0 + q / w) * RW + c0 + q % w;
-    T U4[NV], W4[NV];
-#pragma unroll
-    for (int k = 0; k < NV; k++) U4[k] = s.U[k][id];
-    cons_to_prim(U4, W4);
-#pragma unroll
-    for (int k = 0; k < NV; k++) s.W[k][id] = W4[k];
-  }
-  __syncthreads();
-}
-
+// Registers sized for 4 resident CTAs (the shared-memory limit of both tile
+// shapes): 64 per thread.
 template <class T, int TY, bool HLL>
-__global__ void __launch_bounds__(256) step_kernel(const T* __restrict__ uin, T* __restrict__ uout, int nx, int ny,
+__global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin, T* __restrict__ uout, int nx, int ny,
                                                    int pitch, long long plane, T dx, T dy, T cfl, EulerCtrl* ctrl,
                                                    int p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -179,14 +166,22 @@ __global__ void __launch_bounds__(256) step_kernel(const T* __restrict__ uin, T*
     ctrl->sx[(n + 2) % 3] = 0ull;
     ctrl->sy[(n + 2) % 3] = 0ull;
   }
-  // Region load with wall clamping.
+  // Region load with wall clamping, and the primitives of every region cell
+  // (same thread, so no barrier between them).
   for (int q = threadIdx.x; q < RH * RW; q += blockDim.x) {
     const int r = q / RW, c = q % RW;
     int j = j0 - 2 + r, i = i0 - 2 + c;
     j = j < 0 ? 0 : (j >= ny ? ny - 1 : j);
     i = i < 0 ? 0 : (i >= nx ? nx - 1 : i);
+    T U4[NV], W4[NV];
 #pragma unroll
-    for (int k = 0; k < NV; k++) s.U[k][q] = uin[k * plane + (long long)j * pitch + i];
+    for (int k = 0; k < NV; k++) {
+      U4[k] = uin[k * plane + (long long)j * pitch + i];
+      s.U[k][q] = U4[k];
+    }
+    cons_to_prim(U4, W4);
+#pragma unroll
+    for (int k = 0; k < NV; k++) s.W[k][q] = W4[k];
   }
   __syncthreads();
   const T facx = (T)0.5 * dt / dx, facy = (T)0.5 * dt / dy, rx = dt / dx, ry = dt / dy;
@@ -195,33 +190,37 @@ __global__ void __launch_bounds__(256) step_kernel(const T* __restrict__ uin, T*
   // (the reference's applyBC between the sweeps).
   const int rlo = j0 - 2 < 0 ? 2 - j0 : 0, rhi = j0 - 2 + RH > ny ? ny - (j0 - 2) : RH;  // in-domain rows [rlo, rhi)
   const int clo = i0 - 2 < 0 ? 2 - i0 : 0, chi = i0 - 2 + RW > nx ? nx - (i0 - 2) : RW;
+  // Between the sweeps, a region row (column) beyond a wall holds a copy of
+  // the updated edge row (column); only its primitives are read afterwards,
+  // so they are formed from the edge cell directly.
   if (n % 2 == 0) {
     // x sweep on every region row (columns 2..33), then y sweep on the tile.
-    prims(s, 0, RH, 0, RW);
     sweep<T, TY, 0, HLL>(s, 0, RH, 2, TW + 2, facx, rx);
-    // refresh out-of-domain rows from the updated edge rows
     for (int q = threadIdx.x; q < RH * TW; q += blockDim.x) {
       const int r = q / TW, c = 2 + q % TW;
       const int rs = r < rlo ? rlo : (r >= rhi ? rhi - 1 : r);
-      if (rs != r)
+      T U4[NV], W4[NV];
 #pragma unroll
-        for (int k = 0; k < NV; k++) s.U[k][r * RW + c] = s.U[k][rs * RW + c];
+      for (int k = 0; k < NV; k++) U4[k] = s.U[k][rs * RW + c];
+      cons_to_prim(U4, W4);
+#pragma unroll
+      for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
     }
     __syncthreads();
-    prims(s, 0, RH, 2, TW + 2);
     sweep<T, TY, 1, HLL>(s, 2, TY + 2, 2, TW + 2, facy, ry);
   } else {
-    prims(s, 0, RH, 0, RW);
     sweep<T, TY, 1, HLL>(s, 2, TY + 2, 0, RW, facy, ry);
     for (int q = threadIdx.x; q < TY * RW; q += blockDim.x) {
       const int r = 2 + q / RW, c = q % RW;
       const int cs = c < clo ? clo : (c >= chi ? chi - 1 : c);
-      if (cs != c)
+      T U4[NV], W4[NV];
 #pragma unroll
-        for (int k = 0; k < NV; k++) s.U[k][r * RW + c] = s.U[k][r * RW + cs];
+      for (int k = 0; k < NV; k++) U4[k] = s.U[k][r * RW + cs];
+      cons_to_prim(U4, W4);
+#pragma unroll
+      for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
     }
     __syncthreads();
-    prims(s, 2, TY + 2, 0, RW);
     sweep<T, TY, 0, HLL>(s, 2, TY + 2, 2, TW + 2, facx, rx);
   }
   // Store the tile and reduce the next step's signal speeds.
