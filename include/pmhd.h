@@ -340,7 +340,7 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
                      double* host_out, pmhd_learned_stats* stats);
 
 /* Fine run at `refine` x the coarse resolution, restricted onto the coarse
- * grid at t_end (the judge of the coarse runs); host_out as above. */
+ * grid at t_end (the yardstick of the coarse runs); host_out as above. */
 int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int refine,
                           double* host_out, pmhd_learned_stats* stats);
 

@@ -4,7 +4,7 @@ Fluid Dynamics", 3rd ed. (2009), chapter 4 -- star-region pressure by
 Newton iteration on the pressure function (4.5)-(4.7) from the PV initial
 guess, star velocity (4.9), and sampling of the wave pattern (section 4.5).
 
-TEST INFRASTRUCTURE ONLY: the judge of the 1D Euler kernels' errors, as the
+TEST INFRASTRUCTURE ONLY: the yardstick of the 1D Euler kernels' errors, as the
 reference's analysis/euler/exact_riemann_errors.py is for its solvers.
 """
 import math

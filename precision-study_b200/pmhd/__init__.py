@@ -433,7 +433,7 @@ def _params_arg(params):
 class Learned:
     """Learned coarse-grid correction (a pmhd_learned handle): training pairs
     from the solver, device training, corrected and plain coarse runs, and
-    the fine run that judges them."""
+    the fine run they are measured against."""
 
     def __init__(self, **kw):
         L = load()

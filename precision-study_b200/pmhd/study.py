@@ -12,7 +12,7 @@
         and prints one JSON object: zone-cycles/s of each, and the relative L2
         of every other run against fp64 per conserved variable and per .dat
         primitive column.  The exact-vs-FMA fp64 pair is the rounding noise
-        floor the mixed result is judged against.
+        floor the mixed result is measured against.
 """
 import argparse
 import json
