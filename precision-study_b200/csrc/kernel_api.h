@@ -28,6 +28,8 @@ enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
 // Member::tm and the Batch tile tables; index 0 is the default.
 constexpr int kTileHeights[2] = {16, 8};
 constexpr int kNumTileHeights = 2;
+// A batched stage launch hands its CTAs runs of this many consecutive tiles.
+constexpr int kBatchRun = 16;
 
 // One grid of a batch; lives in device memory (64-byte aligned for the TMA
 // descriptors).

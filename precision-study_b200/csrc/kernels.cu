@@ -102,7 +102,8 @@ static cudaError_t launch_stage_pol(int hlld, int stage, const Batch& b, const M
   if (b.ntiles <= 0) return cudaSuccess;
   const bool batched = single == nullptr;
   if (grid <= 0) grid = sm_count() * occ_pol_ty<Pol, TY>(hlld, batched);
-  if (grid > b.ntiles) grid = b.ntiles;
+  const int units = batched ? (b.ntiles + kBatchRun - 1) / kBatchRun : b.ntiles;  // tiles or runs of tiles
+  if (grid > units) grid = units;
   static const Member empty = {};
   const Member& m0 = batched ? empty : *single;
   if (hlld) {

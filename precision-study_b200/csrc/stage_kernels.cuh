@@ -438,14 +438,32 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
     return;
   }
 
-  // Next tile of this CTA (stride gridDim.x) whose member steps; members
-  // that do not step get their bookkeeping from whoever meets their tile 0.
+  // Tile order.  One grid: tile blockIdx.x, then every gridDim.x-th.  A
+  // batch: runs of kBatchRun consecutive tiles, run blockIdx.x, then
+  // every gridDim.x-th run -- consecutive tiles of a CTA then mostly share
+  // a member, so its descriptor, control slot and step values are re-read
+  // once per member run instead of once per tile, while members that stop
+  // early still leave their tiles spread over all CTAs.
+  auto first_tile = [&]() { return BATCHED ? (int)blockIdx.x * kBatchRun : (int)blockIdx.x; };
+  auto after = [&](int t) {
+    if constexpr (BATCHED)
+      return (t + 1) % kBatchRun != 0 ? t + 1 : t + 1 + ((int)gridDim.x - 1) * kBatchRun;
+    else
+      return t + (int)gridDim.x;
+  };
+  // Next tile of this CTA, from t on, whose member steps; members that do
+  // not step get their bookkeeping from whoever meets their tile 0.
+  int active_mi = -1;  // member last found stepping (batch)
   auto next_active = [&](int t) {
     if constexpr (BATCHED) {
-      for (; t < b.ntiles; t += gridDim.x) {
+      for (; t < b.ntiles; t = after(t)) {
         const int mi = member_of(t);
+        if (mi == active_mi) return t;
         const Member& mm = b.members[mi];
-        if (member_active<Pol, STAGE>(mm, p)) return t;
+        if (member_active<Pol, STAGE>(mm, p)) {
+          active_mi = mi;
+          return t;
+        }
         if (t == tile0_of(mi) && tid == 0) member_bookkeeping<Pol, STAGE>(mm, step_values<Pol, STAGE>(mm, p), p);
       }
       return b.ntiles;
@@ -467,7 +485,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
     fence_barrier_init();
   }
   __syncthreads();
-  int tile = next_active(blockIdx.x);
+  int tile = next_active(first_tile());
   if (tid == 0 && tile < b.ntiles) issue(tile, 0);
   MemberAcc acc = {-1, 0, 0, 0ull};
   StepVals<Pol> v = step_values<Pol, STAGE>(member(BATCHED ? (tile < b.ntiles ? member_of(tile) : 0) : 0), p);
@@ -522,7 +540,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
     const bool checks = !PMHD_FAST_FLUX || !all_usable;
     // The next tile goes into the buffer no thread reads any more: this one
     // (just recovered) or, double-buffered, the previous tile's.
-    const int next = next_active(tile + gridDim.x);
+    const int next = next_active(after(tile));
     if (tid == 0 && next < b.ntiles) {
       fence_proxy_async_smem();  // order earlier reads of that buffer before the async overwrite
       issue(next, (it + 1) % NBUF);
