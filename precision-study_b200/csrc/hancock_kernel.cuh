@@ -92,20 +92,18 @@ __global__ void __launch_bounds__(256, HancockTileOf<Pol>::MINB) hancock_kernel(
   }
   // Region: ghosted rows j0 .. j0+TYH+3, columns i0 .. i0+35 (clamped to the
   // allocation; cells past the domain's ghost ring feed no in-domain update).
+  // The same thread forms the cell's primitives in the storage precision (the
+  // mixed policy's binary64 recovery), kept in the face precision.
   for (int q = tid; q < NR; q += blockDim.x) {
     int gj = j0 + q / RW, gi = i0 + q % RW;
     gj = gj < m.ny + 2 * GHOST ? gj : m.ny + 2 * GHOST - 1;
     gi = gi < m.nx + 2 * GHOST ? gi : m.nx + 2 * GHOST - 1;
-#pragma unroll
-    for (int k = 0; k < NVAR; k++) s.U[k][q] = uin[(size_t)k * m.plane + (size_t)gj * m.pitch + gi];
-  }
-  __syncthreads();
-  // Primitives in the storage precision (the mixed policy's binary64
-  // recovery), kept in the face precision.
-  for (int q = tid; q < NR; q += blockDim.x) {
     S U9[NVAR], P9[NVAR];
 #pragma unroll
-    for (int k = 0; k < NVAR; k++) U9[k] = s.U[k][q];
+    for (int k = 0; k < NVAR; k++) {
+      U9[k] = uin[(size_t)k * m.plane + (size_t)gj * m.pitch + gi];
+      s.U[k][q] = U9[k];
+    }
     recover_cell<Pol>(U9, P9, phS);
 #pragma unroll
     for (int k = 0; k < NVAR; k++) s.P[k][q] = (R)P9[k];
