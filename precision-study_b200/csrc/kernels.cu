@@ -43,8 +43,14 @@ static cudaError_t init_pol() {
 
 template <class Pol, bool HLLD>
 static cudaError_t init_hancock() {
-  return cudaFuncSetAttribute(hancock_kernel<Pol, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(HancockTileOf<Pol>));
+  const int smem = (int)sizeof(HancockTileOf<Pol>);
+  cudaError_t e = cudaFuncSetAttribute(hancock_kernel<Pol, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if constexpr (HancockPersistent<Pol>::on) {
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(hancock_persistent_kernel<Pol, HLLD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem);
+  }
+  return e;
 }
 
 static cudaError_t init() {
@@ -218,12 +224,28 @@ static cudaError_t hancock_pol(int hlld, int part, const Member& m, int parity, 
     return cudaGetLastError();
   }
   constexpr int TYH = HancockTileOf<Pol>::TYH;
-  const unsigned grid = (unsigned)(((m.nx + TX - 1) / TX) * ((m.ny + TYH - 1) / TYH));
+  const int ntiles = ((m.nx + TX - 1) / TX) * ((m.ny + TYH - 1) / TYH);
   const size_t smem = sizeof(HancockTileOf<Pol>);
-  if (hlld)
-    hancock_kernel<Pol, true><<<grid, 256, smem, s>>>(m, parity);
-  else
-    hancock_kernel<Pol, false><<<grid, 256, smem, s>>>(m, parity);
+  if constexpr (HancockPersistent<Pol>::on) {
+    // Persistent: the SMs x the resident CTAs, at most one per tile.
+    static int per_sm = -1;
+    if (per_sm < 0) {
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, hancock_persistent_kernel<Pol, true>, 256, smem);
+      per_sm = nb > 0 ? nb : 1;
+    }
+    int grid = sm_count() * per_sm;
+    if (grid > ntiles) grid = ntiles;
+    if (hlld)
+      hancock_persistent_kernel<Pol, true><<<grid, 256, smem, s>>>(m, parity);
+    else
+      hancock_persistent_kernel<Pol, false><<<grid, 256, smem, s>>>(m, parity);
+  } else {
+    if (hlld)
+      hancock_kernel<Pol, true><<<ntiles, 256, smem, s>>>(m, parity);
+    else
+      hancock_kernel<Pol, false><<<ntiles, 256, smem, s>>>(m, parity);
+  }
   return cudaGetLastError();
 }
 
