@@ -124,6 +124,39 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+class RankOps:
+    """Barrier and max-over-ranks of a multi-process run (torch.distributed:
+    one process per GPU, each advancing its own replica), or no-ops for one
+    process.  device: where the reduction tensor lives ("cuda" under NCCL,
+    "cpu" under gloo)."""
+
+    def __init__(self, dist=None, device="cuda"):
+        self.dist = dist
+        self.device = device
+
+    def barrier(self):
+        if self.dist is None:
+            return
+        if self.device == "cuda":
+            import torch
+            torch.cuda.synchronize()
+        self.dist.barrier()
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def throughput(world, cells, steps, ms):
+    """Whole-job zone-cycles/s: every rank advanced `cells` for `steps` steps
+    and the slowest rank took `ms`."""
+    return world * cells * steps / (ms / 1e3)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -362,19 +395,8 @@ def main():
     n, K, W = args.n, args.steps, args.warmup
     prec = args.precision
 
-    def barrier():
-        if dist is not None:
-            import torch
-            torch.cuda.synchronize()
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ops = RankOps(dist, "cuda")
+    barrier, max_over_ranks = ops.barrier, ops.max
 
     # ---- headline: device-timed throughput of the chosen precision -------
     sampler = ClockSampler(local)
@@ -382,7 +404,7 @@ def main():
     s, st, launches = time_precision(pmhd, prec, n, W, K, local, sampler)
     barrier()
     ms = max_over_ranks(st.device_ms)
-    value = world * n * n * K / (ms / 1e3)
+    value = throughput(world, n * n, K, ms)
     clocks = sampler.summary()
     U_main = s.get_state() if not args.no_compare else None
     s.close()
