@@ -250,6 +250,8 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
 
 int pmhd_learned_num_pairs(const pmhd_learned* L) { return L ? L->npairs : 0; }
 
+}  // extern "C"
+
 namespace {
 
 // Training pairs (before, plain coarse step, restricted fine state at the
@@ -334,6 +336,8 @@ int generate_pairs(pmhd_learned* L, int problem, const double* params, int npara
 }
 
 }  // namespace
+
+extern "C" {
 
 int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
                           int* added) {
