@@ -45,6 +45,14 @@ B_ALG = {"fp64": 360, "mixed": 360, "fp32": 180}
 B_ALG_PER_LAUNCH_CELL = {"fp64": 180, "mixed": 180, "fp32": 90}
 
 
+def aux_steps(K):
+    """Timed steps of the auxiliary Euler and Hancock lines: at least 100 (a
+    20-step region of a 1-2 ms step varies by several per cent between runs),
+    even (their graphs hold step pairs)."""
+    k = max(K, 100)
+    return k + (k & 1)
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
         os.environ.get("LOCAL_RANK", "0"))
@@ -262,13 +270,13 @@ def bench_euler(pmhd, n, W, K, device, max_over_ranks, world):
     for prec in ("fp64", "fp32"):
         with pmhd.Euler2D(n, config=3, precision=prec, device=device) as e:
             e.advance(max_steps=W + (W & 1))
-            st = e.advance(max_steps=K + (K & 1))
+            steps = aux_steps(K)
+            st = e.advance(max_steps=steps)
             ms = max_over_ranks(st.device_ms)
-            steps = K + (K & 1)
             value = world * n * n * steps / (ms / 1e3)
             bpc = 64 if prec == "fp64" else 32
             gbs = bpc * n * n * steps / (ms / 1e3) / 1e9
-            out[prec] = {"value": value, "unit": UNIT, "ms_per_step": ms / steps,
+            out[prec] = {"value": value, "unit": UNIT, "ms_per_step": ms / steps, "timed_steps": steps,
                          "roofline": {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}}
     return out
 
@@ -490,12 +498,12 @@ def main():
             sh = pmhd.Solver(nx=args.hancock, ny=args.hancock, precision=hp, order="hancock", device=local)
             sh.init_problem(pmhd.PROBLEM_ORSZAG_TANG)
             sh.advance(max_steps=W + (W & 1))
-            sth = sh.advance(max_steps=K + (K & 1))
+            sth = sh.advance(max_steps=aux_steps(K))
             msh = max_over_ranks(sth.device_ms)
-            nst = K + (K & 1)
+            nst = aux_steps(K)
             bpc = hancock["algorithmic_bytes_per_zone_cycle"][hp]
             hancock[hp] = {"value": world * args.hancock ** 2 * nst / (msh / 1e3), "unit": UNIT,
-                           "ms_per_step": msh / nst,
+                           "ms_per_step": msh / nst, "timed_steps": nst,
                            "achieved_GBs": bpc * args.hancock ** 2 * nst / (msh / 1e3) / 1e9}
             if hp == "fp64":
                 U64h = sh.get_state()
