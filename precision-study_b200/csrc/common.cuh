@@ -93,6 +93,13 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, uint64_
       : "memory");
 }
 
+// Prefetches a TMA box (same coordinates as tma_load_3d) into L2.
+__device__ __forceinline__ void tma_prefetch_3d(const void* tmap, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(tmap), "r"(x), "r"(y),
+               "r"(z)
+               : "memory");
+}
+
 // Orders this CTA's earlier generic-proxy accesses to shared memory before
 // later async-proxy (TMA) accesses of the same memory.
 __device__ __forceinline__ void fence_proxy_async_smem() {

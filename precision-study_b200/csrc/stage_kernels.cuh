@@ -545,6 +545,9 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
       fence_proxy_async_smem();  // order earlier reads of that buffer before the async overwrite
       issue(next, (it + 1) % NBUF);
     }
+    // Stage 2 also reads U^n of its cells in the update: start bringing this
+    // tile's box of it into L2 now, so the update finds it there.
+    if (STAGE == 2 && tid == 32) tma_prefetch_3d(&m.tm[TI][0], i0, j0, 0);
 
     // ---- interface fluxes --------------------------------------------------
     // Warps 0..TY-1 own one tile row each: lane tx computes the x-interface
