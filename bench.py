@@ -502,9 +502,10 @@ def main():
             msh = max_over_ranks(sth.device_ms)
             nst = aux_steps(K)
             bpc = hancock["algorithmic_bytes_per_zone_cycle"][hp]
+            gbs = bpc * args.hancock ** 2 * nst / (msh / 1e3) / 1e9
             hancock[hp] = {"value": world * args.hancock ** 2 * nst / (msh / 1e3), "unit": UNIT,
                            "ms_per_step": msh / nst, "timed_steps": nst,
-                           "achieved_GBs": bpc * args.hancock ** 2 * nst / (msh / 1e3) / 1e9}
+                           "roofline": {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}}
             if hp == "fp64":
                 U64h = sh.get_state()
             elif hp == "mixed":
