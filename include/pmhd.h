@@ -55,7 +55,7 @@ typedef enum {
   PMHD_ERR_CUDA = 9,         /* CUDA runtime error (code 9)                     */
   PMHD_ERR_TIMEOUT = -1,     /* a bounded device-side wait expired              */
   PMHD_ERR_NOMEM = -2,       /* device allocation failed                        */
-  PMHD_ERR_UNSUPPORTED = -3, /* configuration not supported by this build       */
+  PMHD_ERR_UNSUPPORTED = -3, /* configuration not supported by the library     */
   PMHD_ERR_NODEVICE = -4     /* no CUDA device of compute capability 10.0       */
 } pmhd_status;
 
