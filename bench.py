@@ -209,6 +209,34 @@ def run_reference_cpu(n, instances, t_end=1e-9):
     return instances * n * n / max(walls), walls
 
 
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "mhd2d_glm_gpu_{}")
+
+
+def run_reference_gpu(n, t_end=5.5e-4):
+    """The reference's own GPU programs (its source, recompiled unchanged for
+    sm_100a into oracle/_ref/) on this GPU: Orszag-Tang n x n to a short t_end
+    (40 steps at 4096^2), their own "Time loop wall time" rate.  Output files
+    are suppressed as for the CPU baseline.  None where the binaries are
+    absent."""
+    env = dict(os.environ, OUTDIR="/dev/null/pmhd_no_output")
+    out = {}
+    for prec in ("fp64", "fp32", "mixed"):
+        exe = REF_GPU.format(prec)
+        if not os.path.exists(exe):
+            return None
+        r = subprocess.run([exe, str(n), str(n), repr(t_end), "0.25", "muscl", "hlld", "0.18"], env=env,
+                           capture_output=True, text=True, timeout=300)
+        m = re.search(r"Time loop wall time = ([0-9.eE+-]+) s", r.stdout)
+        k = re.search(r"Steps: (\d+)", r.stdout)
+        if not m or not k:
+            return None
+        steps, wall = int(k.group(1)), float(m.group(1))
+        out[prec] = {"value": n * n * steps / wall, "unit": UNIT, "steps": steps, "wall_s": wall}
+    out["note"] = ("reference src/mhd/mhd2d_glm_gpu.cu (+ _mixed.cu) compiled for sm_100a, OT "
+                   f"{n}x{n}, its own time-loop wall clock")
+    return out
+
+
 def bench_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -540,6 +568,10 @@ def main():
         else:
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": info}
 
+    ref_gpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        ref_gpu = run_reference_gpu(n)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -564,6 +596,11 @@ def main():
             line["euler2d"] = euler
         if hancock is not None:
             line["hancock"] = hancock
+        if ref_gpu is not None:
+            line["reference_gpu_same_box"] = ref_gpu
+            line["speedup_vs_reference_gpu"] = {p: extra[p]["value"] / ref_gpu[p]["value"] if p in extra else
+                                                value / ref_gpu[p]["value"] for p in ("fp64", "fp32", "mixed")
+                                                if p in extra or p == prec}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
