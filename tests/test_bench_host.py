@@ -54,3 +54,24 @@ def test_auxiliary_lines_time_at_least_100_even_steps():
 def test_traffic_comes_from_the_committed_profile():
     t = bench.ncu_traffic("mixed", 1000)
     assert t is not None and 150.0 * 1e6 < t < 200.0 * 1e6  # ~171 B per cell per launch
+
+
+def test_reference_gpu_rates_are_parsed_from_its_stdout(tmp_path, monkeypatch):
+    """run_reference_gpu reads the reference program's own "Done. Steps" and
+    "Time loop wall time" lines (fake programs here print them)."""
+    for prec, wall in (("fp64", "0.902"), ("fp32", "0.494"), ("mixed", "0.876")):
+        exe = tmp_path / f"mhd2d_glm_gpu_{prec}"
+        exe.write_text("#!/bin/sh\n"
+                       "echo 'Done. Steps: 40, final t = 0.00055'\n"
+                       f"echo 'Time loop wall time = {wall} s (744.09 Mcell-steps/s)'\n"
+                       "exit 5\n")
+        exe.chmod(0o755)
+    monkeypatch.setattr(bench, "REF_GPU", str(tmp_path / "mhd2d_glm_gpu_{}"))
+    r = bench.run_reference_gpu(64)
+    assert r["fp64"]["steps"] == 40 and r["fp64"]["value"] == 64 * 64 * 40 / 0.902
+    assert r["mixed"]["wall_s"] == 0.876
+
+
+def test_reference_gpu_absent_gives_none(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "REF_GPU", str(tmp_path / "missing_{}"))
+    assert bench.run_reference_gpu(64) is None
