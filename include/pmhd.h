@@ -392,15 +392,23 @@ int pmhd_euler1d_run(int n, int test, int solver, int precision, int exact, int 
  * mixed, float for fp32; they may be the same buffer); t0 and step0 are the
  * time and step count d_in is at; stream is a cudaStream_t (NULL = the
  * default stream).  The working state lives in one array compiled into the
- * library, PMHD_NOALLOC_SCRATCH_BYTES long, that every GPU loading the
- * library keeps until exit.  Grids whose working state does not fit --
- * 256 + 2 * round_up_256(9 * (ny+4) * round_up(nx+4, 16) * element size)
- * bytes, up to 586^2 cells in fp64/mixed and 828^2 in fp32 -- are rejected
- * with PMHD_ERR_UNSUPPORTED.  All calls share that array: calls that overlap
- * on the GPU race; serialise them.  The first call on a device sets it up
- * (looks up the array's address with that device current); make it before
- * any stream capture.  stats: as pmhd_advance (steps/t are totals including
- * step0/t0; device_ms is not measured, 0). */
+ * library, PMHD_NOALLOC_SCRATCH_BYTES long, that every GPU using this entry
+ * point keeps until exit.  Grids whose working state does not fit --
+ * 2048 + 2 * round_up_256(9 * (ny+4) * round_up(nx+4, 16) * element size)
+ * bytes (a control block and grid descriptor, then two states), up to 586^2
+ * cells in fp64/mixed and 828^2 in fp32 -- are rejected with
+ * PMHD_ERR_UNSUPPORTED.  All calls share that array: calls that overlap on
+ * the GPU race; serialise them.
+ * The array and the kernels' code are placed in device memory when the
+ * CUDA runtime loads this library's device code on a device.  Under lazy
+ * module loading (the CUDA 12 default) that happens during the FIRST call on
+ * each device, which also looks up the array's address with that device
+ * current: that first call does allocate (the array plus the code), so make
+ * it -- for example a one-step call (max_steps = 1) with the same precision,
+ * solver and build on a scratch copy of the state -- before the caller hands
+ * all remaining device memory to its own pool, and before any stream
+ * capture.  Later calls allocate nothing.  stats: as pmhd_advance (steps/t
+ * are totals including step0/t0; device_ms is not measured, 0). */
 #define PMHD_NOALLOC_SCRATCH_BYTES (48u << 20)
 int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, void* d_out, double t0, long long step0,
                          double t_end, long long max_steps, void* stream, pmhd_stats* stats);

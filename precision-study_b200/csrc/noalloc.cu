@@ -14,13 +14,20 @@
 // library (`g_noalloc_scratch`, 48 MiB, see PMHD_NOALLOC_SCRATCH_BYTES).
 //
 // Properties (also stated in include/pmhd.h):
-//   * The array is a static __device__ object: every GPU that loads this
-//     library holds it until the process exits.
-//   * Grids are limited to what fits in it: 256 bytes of control block plus
-//     two states of 9 x (ny + 4) x round_up(nx + 4, 16) elements (8 bytes in
-//     fp64 / mixed, 4 in fp32), each rounded up to 256 bytes.  Up to 586^2
-//     cells in fp64 / mixed and 828^2 in fp32.  Larger grids are rejected
-//     with PMHD_ERR_UNSUPPORTED before anything is launched.
+//   * The array is a static __device__ object: every GPU on which this entry
+//     point runs holds it until the process exits.  The CUDA runtime places
+//     it in device memory when it loads this library's device code on that
+//     GPU; with lazy module loading (the CUDA 12 default) that is the first
+//     call's cudaGetSymbolAddress and first kernel launches, so the FIRST
+//     call on a device allocates (the array and the kernels' code) and must
+//     come before the caller gives the rest of the device memory to its own
+//     pool.  Later calls allocate nothing.
+//   * Grids are limited to what fits in it: kHeadBytes (2048: the control
+//     block and the grid descriptor) plus two states of 9 x (ny + 4) x
+//     round_up(nx + 4, 16) elements (8 bytes in fp64 / mixed, 4 in fp32),
+//     each rounded up to 256 bytes.  Up to 586^2 cells in fp64 / mixed and
+//     828^2 in fp32.  Larger grids are rejected with PMHD_ERR_UNSUPPORTED
+//     before anything is launched.
 //   * Every call shares the array and it keeps the last call's contents;
 //     each call rewrites the control block and the whole state before using
 //     them.  Calls that overlap on the GPU (from several host threads or
@@ -187,18 +194,21 @@ extern "C" int pmhd_advance_noalloc(const pmhd_config* cfg, const void* d_in, vo
       }
     return PMHD_OK;
   };
+  // Chunks of 16 step pairs, each followed by a look at the control block,
+  // so a large step cap used only as a safety bound queues no more launches
+  // than the run needs (steps past the stop condition are no-ops).
   Ctrl r;
-  if (max_steps >= 0) {
-    if ((rc = launch_pairs((max_steps + 1) / 2)) != PMHD_OK) return rc;
+  long long pairs_left = max_steps >= 0 ? (max_steps + 1) / 2 : LLONG_MAX;
+  std::memcpy(&r, &h, sizeof(r));
+  while (pairs_left > 0) {
+    const long long chunk = pairs_left < 16 ? pairs_left : 16;
+    if ((rc = launch_pairs(chunk)) != PMHD_OK) return rc;
+    pairs_left -= chunk;
     PMHD_NA(cudaMemcpyAsync(&r, dctrl, sizeof(r), cudaMemcpyDeviceToHost, s));
     PMHD_NA(cudaStreamSynchronize(s));
-  } else {
-    for (;;) {
-      if ((rc = launch_pairs(16)) != PMHD_OK) return rc;
-      PMHD_NA(cudaMemcpyAsync(&r, dctrl, sizeof(r), cudaMemcpyDeviceToHost, s));
-      PMHD_NA(cudaStreamSynchronize(s));
-      if (r.halted || r.err || r.bad1 != BAD_NONE || r.bad2 != BAD_NONE || !(r.t[0] < r.t_end)) break;
-    }
+    if (r.halted || r.err || r.bad1 != BAD_NONE || r.bad2 != BAD_NONE || !(r.t[0] < r.t_end) ||
+        !(r.step[0] < r.step_limit))
+      break;
   }
   PMHD_NA(kt.soa_to_aos(cfg->precision, dU, plane, nx, ny, pitch, PMHD_LAYOUT_INTERIOR, d_out, s));
   PMHD_NA(cudaStreamSynchronize(s));

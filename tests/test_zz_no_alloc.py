@@ -87,6 +87,40 @@ def test_noalloc_resume_in_place(pmhd_lib):
     np.testing.assert_array_equal(U2, Ur)
 
 
+def test_noalloc_second_call_leaves_device_memory_unchanged(pmhd_lib):
+    """The entry point's promise: once the first call on a device has loaded
+    the library's device code (which places the fixed array in device
+    memory), a call allocates nothing.  Free device memory (cudaMemGetInfo,
+    through torch.cuda.mem_get_info) is read before and after a second call
+    with the same configuration, with the caller's buffers allocated up
+    front."""
+    import torch
+
+    cfg_kwargs = dict(nx=96, ny=80, precision="mixed", exact=False)
+    U0 = _interior(pmhd_lib, 0, **cfg_kwargs)
+    cfg = pmhd_lib.make_config(**cfg_kwargs)
+    d_in = torch.from_numpy(U0).cuda()
+    d_out = torch.empty_like(d_in)
+    lib = pmhd_lib.load()
+    st = pmhd_lib.Stats()
+
+    def call():
+        rc = lib.pmhd_advance_noalloc(ctypes.byref(cfg), d_in.data_ptr(), d_out.data_ptr(), 0.0, 0, 0.05, -1,
+                                      None, ctypes.byref(st))
+        torch.cuda.synchronize()
+        return rc
+
+    assert call() == pmhd_lib.OK  # first call on this device: sets up, may load code
+    first = d_out.cpu().numpy()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    assert call() == pmhd_lib.OK
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, (free_before, free_after)
+    np.testing.assert_array_equal(d_out.cpu().numpy(), first)
+    assert st.steps > 0
+
+
 def test_noalloc_rejects_grids_beyond_the_fixed_scratch(pmhd_lib):
     cfg = pmhd_lib.make_config(nx=1024, ny=1024, precision="fp64")
     st = pmhd_lib.Stats()
