@@ -39,6 +39,11 @@ struct Ctrl {
   unsigned long long degenerate, nonphysical;  // HLLD fallbacks this advance
   unsigned long long active_stage_launches;    // stage launches that did work
   double t_bad;                 // time at the start of the failing step (Hancock)
+  // Test hook of the bounded-wait path, 0 in normal runs.  When > 0, a
+  // one-grid stage launch issues no input load for its first tile and waits
+  // for it at most this many polls, so every CTA takes the wait-expired exit
+  // with nothing in flight.  Set by the host from PMHD_TEST_STALL_POLLS.
+  int test_stall;
 };
 
 enum DeviceErr : int { DERR_NONE = 0, DERR_TMA_TIMEOUT = 1 };

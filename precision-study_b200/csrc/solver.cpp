@@ -14,6 +14,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -389,6 +390,12 @@ int pmhd_advance(pmhd_solver* s, double t_end, long long max_steps, pmhd_stats* 
   h.t_end = to_time_type(s, t_end);
   h.step_limit = max_steps < 0 ? LLONG_MAX : s->steps + max_steps;
   h.bad1 = h.bad2 = BAD_NONE;
+  // Test hook of the bounded-wait error path (see Ctrl::test_stall): the
+  // SSPRK2 stage kernels time out on purpose, with no load in flight.
+  if (const char* e = std::getenv("PMHD_TEST_STALL_POLLS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    h.test_stall = (v > 0 && v < (1L << 20)) ? (int)v : 0;
+  }
   PMHD_CU(cudaMemcpyAsync(s->dCtrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, s->stream));
   PMHD_CU(cudaEventRecord(s->ev0, s->stream));
   // CFL speed of the initial state; later steps get it from stage 2.

@@ -485,8 +485,10 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
     fence_barrier_init();
   }
   __syncthreads();
+  // Test hook (Ctrl::test_stall): no first load, a short wait, the error exit.
+  const int stall = BATCHED ? 0 : m0.ctrl->test_stall;
   int tile = next_active(first_tile());
-  if (tid == 0 && tile < b.ntiles) issue(tile, 0);
+  if (tid == 0 && tile < b.ntiles && stall == 0) issue(tile, 0);
   MemberAcc acc = {-1, 0, 0, 0ull};
   StepVals<Pol> v = step_values<Pol, STAGE>(member(BATCHED ? (tile < b.ntiles ? member_of(tile) : 0) : 0), p);
 
@@ -506,10 +508,12 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
     const int cb = it % NBUF;                        // buffer of this tile
     const uint32_t par = (uint32_t)(it / NBUF) & 1;  // its mbarrier phase
     S* sU = ubuf(cb);
-    const bool got = __syncthreads_and(mbar_wait_bounded(&bar[cb], par, kWaitIters));
+    const bool got =
+        __syncthreads_and(mbar_wait_bounded(&bar[cb], par, stall > 0 ? (uint32_t)stall : kWaitIters));
     if (!got) {
       if (tid == 0) atomicExch(&m.ctrl->err, (int)DERR_TMA_TIMEOUT);
-      mbar_wait_bounded(&bar[cb], par, kWaitIters);  // let the copy land before leaving
+      // Let an issued copy land before leaving (the test hook issued none).
+      if (stall == 0) mbar_wait_bounded(&bar[cb], par, kWaitIters);
       return;
     }
 

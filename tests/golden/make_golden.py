@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Needs the reference tree (default /root/reference) and its CPU programs
-built by `make -C oracle ref` into oracle/_ref/.  Writes:
+Needs the reference's CPU programs built from its source tree by
+`make -C oracle ref REF=<tree>` (or with PMHD_REF=<tree> in the environment)
+into oracle/_ref/.  Writes:
 
   point_fp64.npz, point_fp32.npz, point_gamma2_fp64.npz
       inputs and outputs of the reference's header-only point functions
@@ -16,8 +17,13 @@ built by `make -C oracle ref` into oracle/_ref/.  Writes:
       non-'#' lines of the .dat output) and summary numbers of the reference
       CPU solver src/mhd/mhd2d_glm_cpu.cpp on small Orszag-Tang grids, fp64
       and fp32, all order/solver combinations.
+  runs_large.json  (--large; about five minutes of CPU per run)
+      the same for the plain-method configuration Orszag-Tang 256^2 to
+      t = 0.5 (MUSCL, HLLD, CFL 0.25, alpha 0.18), fp64 and fp32, and the
+      reference's failure report (exit code, step, cell) of a run that meets
+      a non-physical stage.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [--large]
 """
 import hashlib
 import json
@@ -195,8 +201,62 @@ def make_run_fixtures():
                    "built -O2 -DMHD_HLLD_TOLERANCE_VALUE=1.0e-4 (oracle/Makefile)", "runs": out}, f, indent=1)
 
 
+def _run_summary(stdout, path):
+    steps = int(re.search(r"Steps: (\d+)", stdout).group(1))
+    m = re.search(r"degenerate=(\d+), nonphysical=(\d+)", stdout)
+    ev = re.search(r"HLLD flux evaluations = (\d+) \(x=(\d+), y=(\d+)\)", stdout)
+    dv = re.search(r"divB L1 = ([0-9.eE+-]+), divB Linf = ([0-9.eE+-]+), psi Linf = ([0-9.eE+-]+)", stdout)
+    return {"steps": steps, "ch_last_printed": float(re.search(r"c_h\(last\) = ([0-9.eE+-]+)", stdout).group(1)),
+            "degenerate": int(m.group(1)), "nonphysical": int(m.group(2)),
+            "x_evals": int(ev.group(2)), "y_evals": int(ev.group(3)),
+            "divb_line": dv.group(0) if dv else None, "md5": data_md5(path)}
+
+
+# A run that meets a non-physical state: first order, HLLD, CFL 0.95 and
+# alpha 0.01 on Orszag-Tang 32^2 (the reference stops in stage 1 of step 15).
+FAILING = (32, 32, 0.5, 0.95, "first", "hlld", 0.01)
+
+
+def make_large_run_fixtures():
+    out = {"generator": "tests/golden/make_golden.py --large",
+           "reference": "src/mhd/mhd2d_glm_cpu.cpp built -O2 -DMHD_HLLD_TOLERANCE_VALUE=1.0e-4 (oracle/Makefile)",
+           "runs": [], "failures": []}
+    with tempfile.TemporaryDirectory() as d:
+        procs = []
+        for prec in ("fp64", "fp32"):
+            binary = os.path.join(REF_DIR, f"mhd2d_glm_cpu_{prec}")
+            env = dict(os.environ, OUTDIR=os.path.join(d, prec))
+            args = [binary, "256", "256", "0.5", "0.25", "muscl", "hlld", "0.18"]
+            procs.append((prec, subprocess.Popen(args, stdout=subprocess.PIPE, text=True, env=env)))
+        for prec, p in procs:
+            stdout, _ = p.communicate()
+            assert p.returncode == 0, prec
+            fn = os.path.join(d, prec, f"orszag_tang_glm_muscl_hlld_{prec}_N256x256.dat")
+            rec = {"precision": prec, "nx": 256, "ny": 256, "t_end": 0.5, "cfl": 0.25, "order": "muscl",
+                   "solver": "hlld", "alpha": 0.18}
+            rec.update(_run_summary(stdout, fn))
+            out["runs"].append(rec)
+            print(rec)
+        for prec in ("fp64", "fp32"):
+            binary = os.path.join(REF_DIR, f"mhd2d_glm_cpu_{prec}")
+            nx, ny, t_end, cfl, order, solver, alpha = FAILING
+            r = subprocess.run([binary, str(nx), str(ny), repr(t_end), repr(cfl), order, solver, repr(alpha)],
+                               capture_output=True, text=True, env=dict(os.environ, OUTDIR=d))
+            m = re.search(r"Error: (non-physical RK stage|non-physical state) at step (\d+), cell \((\d+), (\d+)\)",
+                          r.stderr)
+            rec = {"precision": prec, "args": [nx, ny, t_end, cfl, order, solver, alpha], "exit": r.returncode,
+                   "message": m.group(0), "step": int(m.group(2)), "i": int(m.group(3)), "j": int(m.group(4))}
+            out["failures"].append(rec)
+            print(rec)
+    with open(os.path.join(OUT, "runs_large.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
     if not os.path.exists(os.path.join(REF_DIR, "ref_point_fp64")):
         sys.exit("build the reference programs first: make -C oracle ref")
-    make_point_fixtures()
-    make_run_fixtures()
+    if "--large" in sys.argv[1:]:
+        make_large_run_fixtures()
+    else:
+        make_point_fixtures()
+        make_run_fixtures()

@@ -145,6 +145,55 @@ def test_exact_ot192_matches_reference_output(pmhd_lib, prec, tmp_path):
     assert _md5_data_lines(path) == ka["md5"]
 
 
+def _large_runs():
+    import json
+    here = os.path.dirname(os.path.abspath(__file__))
+    return json.load(open(os.path.join(here, "golden", "runs_large.json")))["runs"]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_exact_ot256_plain_method_matches_reference_output(pmhd_lib, prec, tmp_path):
+    """The plain-method configuration (Orszag-Tang 256^2, MUSCL + HLLD, CFL
+    0.25, alpha 0.18, to t = 0.5): the exact build's .dat data lines equal
+    the reference CPU program's, bit for bit (md5 written by the reference
+    program, tests/golden/runs_large.json), with the same step count, c_h and
+    HLLD counters."""
+    g = [r for r in _large_runs() if r["precision"] == prec][0]
+    with pmhd_lib.Solver(nx=256, ny=256, precision=prec, exact=True) as s:
+        s.init_problem(0)
+        st = s.advance(t_end=0.5)
+        path = str(tmp_path / s.dat_filename())
+        s.write_dat(path)
+    assert st.steps == g["steps"]
+    assert float("%g" % st.ch_last) == g["ch_last_printed"]
+    assert (st.degenerate, st.nonphysical) == (g["degenerate"], g["nonphysical"])
+    assert (st.x_evals, st.y_evals) == (g["x_evals"], g["y_evals"])
+    assert _md5_data_lines(path) == g["md5"]
+
+
+def test_fma_fp64_full_ot192_within_1e12_of_the_reference_arithmetic(pmhd_lib):
+    """North-star bar for the FMA build: relative L2 <= 1e-12 per variable
+    against the reference CPU fp64 result, on the reference's own FMA-effect
+    comparison (Orszag-Tang 192^2 to t = 0.5; the reference measured 6.41e-13
+    for its GPU FMA build, logs/mhd/gpu_backend_20260718/
+    cmp_gpu_fma_effect_N192.txt).  The exact build stands in for the CPU
+    result: test_exact_ot192_matches_reference_output pins it to the CPU
+    program's output md5."""
+    with pmhd_lib.Solver(nx=192, ny=192, precision="fp64", exact=True) as s:
+        s.init_problem(0)
+        se = s.advance(t_end=0.5)
+        Ue = s.get_state()
+    with pmhd_lib.Solver(nx=192, ny=192, precision="fp64", exact=False) as s:
+        s.init_problem(0)
+        sf = s.advance(t_end=0.5)
+        Uf = s.get_state()
+    assert se.steps == sf.steps == 1936
+    # The reference's comparison runs over the .dat columns rho vx vy vz p Bx
+    # By Bz E (analysis/mhd/compare_precision.py:51-58).
+    rel = pmhd_lib.relative_l2(pmhd_lib.conserved_to_dat_columns(Ue), pmhd_lib.conserved_to_dat_columns(Uf))
+    assert np.all(rel <= 1e-12), rel
+
+
 # Reference CPU logs logs/mhd/ot_large_eps1e-4_20260715/ot_fp{64,32}_N{256,384,512}.log
 OT_LARGE = [
     ("fp64", 256, 2595, 37374, 8), ("fp64", 384, 3917, 144924, 4), ("fp64", 512, 5239, 374612, 20),

@@ -178,3 +178,34 @@ def test_mixed_oracle_close_to_f64(oracle):
     d = Ua[2:-2, 2:-2, :8] - Ub[2:-2, 2:-2, :8]
     rel = np.sqrt((d ** 2).mean(axis=(0, 1))) / np.maximum(np.sqrt((Ua[2:-2, 2:-2, :8] ** 2).mean(axis=(0, 1))), 1e-30)
     assert np.all(rel[[0, 1, 2, 4, 5, 6]] < 1e-5), rel
+
+
+LARGE = json.load(open(os.path.join(GOLD, "runs_large.json")))
+
+
+@pytest.mark.parametrize("fail", LARGE["failures"], ids=lambda r: r["precision"])
+def test_oracle_failure_report_matches_reference(oracle, fail):
+    """The oracle stops where the reference CPU program stops on a run that
+    meets a non-physical stage: same status (exit code), step and first bad
+    cell (tests/golden/runs_large.json, written by the reference program)."""
+    nx, ny, t_end, cfl, order, solver, alpha = fail["args"]
+    prec = "f32" if fail["precision"] == "fp32" else "f64"
+    cfg = oracle.make_config(nx, ny, t_end, cfl=cfl, alpha=alpha, muscl=order == "muscl", hlld=solver == "hlld")
+    U = oracle.init_ref_problem(prec, 0, nx, ny)
+    st = oracle.run(prec, cfg, U)
+    assert st.status == fail["exit"]
+    assert (st.steps, st.bad_i, st.bad_j) == (fail["step"], fail["i"], fail["j"])
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("run", LARGE["runs"], ids=lambda r: r["precision"])
+def test_oracle_ot256_matches_reference_output(oracle, run, tmp_path):
+    """The plain-method configuration (Orszag-Tang 256^2 to t = 0.5): the
+    oracle reproduces the reference program's step count, counters and
+    data-line md5 (about ten minutes of CPU)."""
+    prec = "f32" if run["precision"] == "fp32" else "f64"
+    cfg = oracle.make_config(256, 256, 0.5)
+    U = oracle.init_ref_problem(prec, 0, 256, 256)
+    st = oracle.run(prec, cfg, U)
+    assert (st.steps, st.degenerate, st.nonphysical) == (run["steps"], run["degenerate"], run["nonphysical"])
+    assert oracle.dat_lines_md5(prec, cfg, U, str(tmp_path / "o.dat")) == run["md5"]
