@@ -83,12 +83,21 @@ class ClockSampler:
         self._stop = threading.Event()
         self._thread = None
         self._handle = None
+        self._lock = threading.Lock()
+        self._smax = None
 
     def mark_start(self):
         self.t0 = time.time()
 
     def mark_end(self):
         self.t1 = time.time()
+        # The sampling thread may have been starved during a short region; a
+        # sample taken here, on the caller's thread, closes the bracket.
+        if self._handle is not None:
+            try:
+                self._sample()
+            except Exception as exc:
+                self.error = self.error or repr(exc)
 
     def _open(self):
         nv = self.nvml
@@ -113,13 +122,15 @@ class ClockSampler:
 
     def _sample(self):
         nv, h = self.nvml, self._handle
-        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        try:
-            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-        except AttributeError:
-            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
-        self.rows.append((time.time(), float(sm), float(smax), int(bits)))
+        with self._lock:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            if self._smax is None:
+                self._smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            try:
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except AttributeError:
+                bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.rows.append((time.time(), float(sm), self._smax, int(bits)))
 
     def _run(self):
         while True:
@@ -171,10 +182,13 @@ class ClockSampler:
                 if bit and (r[3] & bit):
                     reasons.add(name)
         sm = [r[1] for r in used]
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": used[0][2] if used else None,
-                "samples": len(rows), "samples_in_region": len(inside),
-                "region_s": (t1 - t0) if self.t0 is not None and self.t1 is not None else None,
-                "reasons": sorted(reasons), "source": "nvml"}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": used[0][2] if used else None,
+               "samples": len(rows), "samples_in_region": len(inside),
+               "region_s": (t1 - t0) if self.t0 is not None and self.t1 is not None else None,
+               "reasons": sorted(reasons), "source": "nvml"}
+        if self.error:
+            out["sampler_error"] = self.error
+        return out
 
 
 class RankOps:

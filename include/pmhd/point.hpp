@@ -43,14 +43,16 @@ enum HlldStatus : int { HLLD_OK = 0, HLLD_FALLBACK_DEGENERATE = 1, HLLD_FALLBACK
 
 template <class T>
 struct Phys {
-  T gamma;  // ratio of specific heats
-  T gm1;    // gamma - 1, evaluated as (gamma - 1) in T
-  T tol;    // HLLD relative degeneracy tolerance
+  T gamma;    // ratio of specific heats
+  T gm1;      // gamma - 1, evaluated as (gamma - 1) in T
+  T tol;      // HLLD relative degeneracy tolerance
+  T inv_gm1;  // 1 / gm1 (performance-build forms only)
   PMHD_HD static Phys make(double g, double tolerance) {
     Phys p;
     p.gamma = (T)g;
     p.gm1 = p.gamma - (T)1.0;
     p.tol = (T)tolerance;
+    p.inv_gm1 = (T)1.0 / p.gm1;
     return p;
   }
 };
@@ -598,6 +600,387 @@ PMHD_HD T cell_speed(const T* P, const Phys<T>& ph) {
   const T sx = vabs(P[MX]) + fast_speed<T, 0>(P, ph);
   const T sy = vabs(P[MY]) + fast_speed<T, 1>(P, ph);
   return vmax(sx, sy);
+}
+
+// ---- performance-build forms ------------------------------------------------
+//
+// The kernels of the performance build (never the parity build) use the forms
+// below: the same HLLD / HLL + GLM algorithm, rearranged so a GPU thread issues
+// fewer instructions.  Equal to the reference forms above up to rounding:
+//   * reciprocals instead of divisions: one per density, wave-speed
+//     difference and denominator, shared by every quotient of that divisor
+//     (binary32: the hardware's approximate reciprocal, <= 1 ulp);
+//   * the Riemann problem is posed on primitives plus total energy: the face
+//     primitives of the reconstruction go in directly (the reference forms
+//     conserved states and recovers primitives again), the pressure carries
+//     the GLM change of B_n as gm1 (B_n^2 - B_n*^2) / 2 (what the recovery of
+//     the modified conserved state gives), and a conserved component is
+//     formed only where a flux difference needs it;
+//   * the field-smallness guard |B_n| <= tol sqrt(max(b2L, b2R)) is tested
+//     squared, and the star-state positivity tests use the star primitives at
+//     hand (as the FAST forms above).
+
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float fast_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float fast_rsqrt(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float fast_sqrt(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+#else
+inline float fast_rcp(float x) { return 1.0f / x; }
+inline float fast_rsqrt(float x) { return 1.0f / std::sqrt(x); }
+inline float fast_sqrt(float x) { return std::sqrt(x); }
+#endif
+PMHD_HD double fast_rcp(double x) { return 1.0 / x; }
+PMHD_HD double fast_rsqrt(double x) { return 1.0 / vsqrt(x); }
+PMHD_HD double fast_sqrt(double x) { return vsqrt(x); }
+
+// Binary64 reciprocal by two Newton-Raphson steps r <- r + r (1 - x r) from
+// the binary32 approximate reciprocal (relative error ~2^-22 -> ~2^-44 ->
+// below binary64 rounding); for 1e-30 < |x| < 1e30.
+PMHD_HD double rcp_newton(double x) {
+#if defined(__CUDA_ARCH__)
+  double r = (double)fast_rcp((float)x);
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+#else
+  return 1.0 / x;
+#endif
+}
+
+// GLM constants of one stage, uniform over a launch: ch, max(ch, 1e-12),
+// 0.5 / max(ch, 1e-12) and ch^2.
+template <class T>
+struct GlmK {
+  T ch, ch_safe, half_inv, ch2;
+  PMHD_HD static GlmK make(T c) {
+    GlmK k;
+    k.ch = c;
+    k.ch_safe = vmax(c, (T)1.0e-12);
+    k.half_inv = (T)0.5 / k.ch_safe;
+    k.ch2 = c * c;
+    return k;
+  }
+};
+
+// One side of an interface in normal/tangential components, after the GLM
+// substitution B_n := B_n*.
+template <class T>
+struct RSide {
+  T rho, inv, vn, vt1, vt2, p, bt1, bt2, e, bt2s;  // bt2s = bt1^2 + bt2^2
+};
+
+template <class T, int AX>
+PMHD_HD RSide<T> rside(const T* P, T bn0, T bns, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  RSide<T> s;
+  s.rho = vmax(P[RHO], rho_floor<T>());
+  s.inv = fast_rcp(s.rho);
+  s.vn = P[D::vn];
+  s.vt1 = P[D::vt1];
+  s.vt2 = P[D::vt2];
+  s.bt1 = P[D::bt1];
+  s.bt2 = P[D::bt2];
+  s.bt2s = s.bt1 * s.bt1 + s.bt2 * s.bt2;
+  const T v2 = s.vn * s.vn + s.vt1 * s.vt1 + s.vt2 * s.vt2;
+  const T p0 = P[EN];
+  s.e = p0 * ph.inv_gm1 + (T)0.5 * s.rho * v2 + (T)0.5 * (bn0 * bn0 + s.bt2s);
+  s.p = p0 + (T)0.5 * ph.gm1 * (bn0 - bns) * (bn0 + bns);
+  return s;
+}
+
+// Fast magnetosonic speed along the normal (fast_speed with one reciprocal).
+template <class T>
+PMHD_HD T rside_cf(const RSide<T>& s, T bn2, const Phys<T>& ph) {
+  const T a2 = ph.gamma * vmax(s.p, p_floor<T>()) * s.inv;
+  const T b2 = (bn2 + s.bt2s) * s.inv;
+  const T can2 = bn2 * s.inv;
+  const T sum = a2 + b2;
+  const T disc = vmax(sum * sum - (T)4.0 * a2 * can2, (T)0.0);
+  return fast_sqrt(vmax((T)0.5 * (sum + fast_sqrt(disc)), (T)0.0));
+}
+
+// Physical flux of one side (slots in AX order; F[B_n] is left to the caller).
+template <class T, int AX>
+PMHD_HD void rside_flux(const RSide<T>& s, T bn, T bn2, T* F) {
+  using D = Dir<AX>;
+  const T ptot = s.p + (T)0.5 * (bn2 + s.bt2s);
+  const T vdotb = s.vn * bn + s.vt1 * s.bt1 + s.vt2 * s.bt2;
+  const T mn = s.rho * s.vn;
+  F[RHO] = mn;
+  F[D::vn] = mn * s.vn + ptot - bn2;
+  F[D::vt1] = mn * s.vt1 - bn * s.bt1;
+  F[D::vt2] = mn * s.vt2 - bn * s.bt2;
+  F[EN] = (s.e + ptot) * s.vn - bn * vdotb;
+  F[D::bt1] = s.vn * s.bt1 - bn * s.vt1;
+  F[D::bt2] = s.vn * s.bt2 - bn * s.vt2;
+}
+
+// HLL along AX from two sides and their outer wave speeds sL < 0 < sR.
+template <class T, int AX>
+PMHD_HD void rside_hll(const RSide<T>& L, const RSide<T>& R, T bn, T bn2, T sL, T sR, T* F) {
+  using D = Dir<AX>;
+  T FL[NV8], FR[NV8];
+  rside_flux<T, AX>(L, bn, bn2, FL);
+  rside_flux<T, AX>(R, bn, bn2, FR);
+  const T inv = fast_rcp(sR - sL);
+  const T ss = sL * sR;
+  F[RHO] = (sR * FL[RHO] - sL * FR[RHO] + ss * (R.rho - L.rho)) * inv;
+  F[D::vn] = (sR * FL[D::vn] - sL * FR[D::vn] + ss * (R.rho * R.vn - L.rho * L.vn)) * inv;
+  F[D::vt1] = (sR * FL[D::vt1] - sL * FR[D::vt1] + ss * (R.rho * R.vt1 - L.rho * L.vt1)) * inv;
+  F[D::vt2] = (sR * FL[D::vt2] - sL * FR[D::vt2] + ss * (R.rho * R.vt2 - L.rho * L.vt2)) * inv;
+  F[EN] = (sR * FL[EN] - sL * FR[EN] + ss * (R.e - L.e)) * inv;
+  F[D::bt1] = (sR * FL[D::bt1] - sL * FR[D::bt1] + ss * (R.bt1 - L.bt1)) * inv;
+  F[D::bt2] = (sR * FL[D::bt2] - sL * FR[D::bt2] + ss * (R.bt2 - L.bt2)) * inv;
+}
+
+// Star state of one side (hlld_star): density, tangential velocity and field,
+// energy, and v.B; returns the status.
+template <class T>
+struct RStar {
+  T rho, vt1, vt2, bt1, bt2, e, vb;
+};
+
+template <class T>
+PMHD_HD int rside_star(const RSide<T>& s, T sw, T sm, T pt, T pts, T bn, T bn2, RStar<T>& o, const Phys<T>& ph) {
+  const T smv = sw - s.vn;
+  const T sms = sw - sm;
+  if (hlld_small(sms, vmax(vabs(sw), vabs(sm)), ph)) return HLLD_FALLBACK_DEGENERATE;
+  const T inv_sms = fast_rcp(sms);
+  const T d = s.rho * smv;
+  o.rho = d * inv_sms;
+  if (o.rho <= rho_floor<T>()) return HLLD_FALLBACK_NONPHYSICAL;
+  const T dsms = d * sms;
+  const T denom = dsms - bn2;
+  if (hlld_small(denom, vabs(dsms) + bn2, ph)) return HLLD_FALLBACK_DEGENERATE;
+  const T inv_den = fast_rcp(denom);
+  const T cb = bn * (sm - s.vn) * inv_den;
+  const T fb = (d * smv - bn2) * inv_den;
+  o.vt1 = s.vt1 - s.bt1 * cb;
+  o.vt2 = s.vt2 - s.bt2 * cb;
+  o.bt1 = s.bt1 * fb;
+  o.bt2 = s.bt2 * fb;
+  const T vdotb = s.vn * bn + s.vt1 * s.bt1 + s.vt2 * s.bt2;
+  o.vb = sm * bn + o.vt1 * o.bt1 + o.vt2 * o.bt2;
+  o.e = (smv * s.e - pt * s.vn + pts * sm + bn * (vdotb - o.vb)) * inv_sms;
+  const T v2 = sm * sm + o.vt1 * o.vt1 + o.vt2 * o.vt2;
+  const T b2 = bn2 + o.bt1 * o.bt1 + o.bt2 * o.bt2;
+  const T ps = ph.gm1 * (o.e - (T)0.5 * o.rho * v2 - (T)0.5 * b2);
+  return (ps > p_floor<T>()) ? HLLD_OK : HLLD_FALLBACK_NONPHYSICAL;
+}
+
+// F += sw (Us - U) for one side (slots in AX order; the B_n jump is zero).
+template <class T, int AX>
+PMHD_HD void rside_jump(const RSide<T>& s, const RStar<T>& st, T sm, T sw, T* F) {
+  using D = Dir<AX>;
+  F[RHO] += sw * (st.rho - s.rho);
+  F[D::vn] += sw * (st.rho * sm - s.rho * s.vn);
+  F[D::vt1] += sw * (st.rho * st.vt1 - s.rho * s.vt1);
+  F[D::vt2] += sw * (st.rho * st.vt2 - s.rho * s.vt2);
+  F[EN] += sw * (st.e - s.e);
+  F[D::bt1] += sw * (st.bt1 - s.bt1);
+  F[D::bt2] += sw * (st.bt2 - s.bt2);
+}
+
+// F += sws (UD - Us) (density and normal momentum do not jump).
+template <class T, int AX>
+PMHD_HD void rside_jump2(const RStar<T>& st, T vt1D, T vt2D, T bt1D, T bt2D, T eD, T sws, T* F) {
+  using D = Dir<AX>;
+  const T sr = sws * st.rho;
+  F[D::vt1] += sr * (vt1D - st.vt1);
+  F[D::vt2] += sr * (vt2D - st.vt2);
+  F[EN] += sws * (eD - st.e);
+  F[D::bt1] += sws * (bt1D - st.bt1);
+  F[D::bt2] += sws * (bt2D - st.bt2);
+}
+
+// One side from a 9-slot CONSERVED state (the Riemann problem of evolved
+// conserved faces): the recovery cons_to_prim performs on the state with
+// B_n := B_n*, with one reciprocal of the density.
+template <class T, int AX>
+PMHD_HD RSide<T> rside_cons(const T* U, T bns, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  RSide<T> s;
+  s.rho = vmax(U[RHO], rho_floor<T>());
+  s.inv = fast_rcp(s.rho);
+  s.vn = U[D::vn] * s.inv;
+  s.vt1 = U[D::vt1] * s.inv;
+  s.vt2 = U[D::vt2] * s.inv;
+  s.bt1 = U[D::bt1];
+  s.bt2 = U[D::bt2];
+  s.bt2s = s.bt1 * s.bt1 + s.bt2 * s.bt2;
+  const T v2 = s.vn * s.vn + s.vt1 * s.vt1 + s.vt2 * s.vt2;
+  s.e = U[EN];
+  s.p = ph.gm1 * (s.e - (T)0.5 * s.rho * v2 - (T)0.5 * (bns * bns + s.bt2s));
+  return s;
+}
+
+template <class T, int AX>
+PMHD_HD int hlld_core_fast(const RSide<T>& L, const RSide<T>& R, T bn, bool use_hlld, T* F, const Phys<T>& ph);
+
+// GLM + HLLD (or HLL) interface flux along AX from the two face primitives
+// (9 slots as reconstructed): the performance-build form of glm_flux /
+// glm_flux_prim, same statuses.  F receives all nine slots.
+template <class T, int AX>
+PMHD_HD int glm_flux_fast(const T* PL, const T* PR, const GlmK<T>& g, bool use_hlld, T* F, const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T bnL0 = PL[D::bn], bnR0 = PR[D::bn], psiL = PL[PSI], psiR = PR[PSI];
+  const T bn = (T)0.5 * (bnL0 + bnR0) - (psiR - psiL) * g.half_inv;
+  F[D::bn] = (T)0.5 * (psiL + psiR) - (T)0.5 * g.ch_safe * (bnR0 - bnL0);
+  F[PSI] = g.ch2 * bn;
+  return hlld_core_fast<T, AX>(rside<T, AX>(PL, bnL0, bn, ph), rside<T, AX>(PR, bnR0, bn, ph), bn, use_hlld, F,
+                               ph);
+}
+
+// The same from the two 9-slot conserved face states (performance-build form
+// of glm_flux).
+template <class T, int AX>
+PMHD_HD int glm_flux_fast_cons(const T* UL, const T* UR, const GlmK<T>& g, bool use_hlld, T* F,
+                               const Phys<T>& ph) {
+  using D = Dir<AX>;
+  const T bnL0 = UL[D::bn], bnR0 = UR[D::bn], psiL = UL[PSI], psiR = UR[PSI];
+  const T bn = (T)0.5 * (bnL0 + bnR0) - (psiR - psiL) * g.half_inv;
+  F[D::bn] = (T)0.5 * (psiL + psiR) - (T)0.5 * g.ch_safe * (bnR0 - bnL0);
+  F[PSI] = g.ch2 * bn;
+  return hlld_core_fast<T, AX>(rside_cons<T, AX>(UL, bn, ph), rside_cons<T, AX>(UR, bn, ph), bn, use_hlld, F, ph);
+}
+
+// HLLD (or HLL) on the eight MHD slots between two sides sharing the normal
+// field bn; writes every slot of F but B_n and psi.
+template <class T, int AX>
+PMHD_HD int hlld_core_fast(const RSide<T>& L, const RSide<T>& R, T bn, bool use_hlld, T* F, const Phys<T>& ph) {
+  const T bn2 = bn * bn;
+  const T cfL = rside_cf<T>(L, bn2, ph), cfR = rside_cf<T>(R, bn2, ph);
+  const T sL = vmin(L.vn - cfL, R.vn - cfR);
+  const T sR = vmax(L.vn + cfL, R.vn + cfR);
+  if (sL >= (T)0.0) {
+    rside_flux<T, AX>(L, bn, bn2, F);
+    return HLLD_OK;
+  }
+  if (sR <= (T)0.0) {
+    rside_flux<T, AX>(R, bn, bn2, F);
+    return HLLD_OK;
+  }
+  int status = HLLD_OK;
+  if (use_hlld) {
+    do {
+      const T b2L = bn2 + L.bt2s, b2R = bn2 + R.bt2s;
+      const T ptL = vmax(L.p, p_floor<T>()) + (T)0.5 * b2L;
+      const T ptR = vmax(R.p, p_floor<T>()) + (T)0.5 * b2R;
+      const T dL = L.rho * (sL - L.vn), dR = R.rho * (sR - R.vn);
+      const T denom_sm = dR - dL;
+      if (hlld_small(denom_sm, vabs(dR) + vabs(dL), ph) || bn2 <= ph.tol * ph.tol * vmax(b2L, b2R)) {
+        status = HLLD_FALLBACK_DEGENERATE;
+        break;
+      }
+      const T sm = (dR * R.vn - dL * L.vn + ptL - ptR) * fast_rcp(denom_sm);
+      const T pts = (T)0.5 * ((ptL + dL * (sm - L.vn)) + (ptR + dR * (sm - R.vn)));
+      RStar<T> Ls, Rs;
+      const int stL = rside_star<T>(L, sL, sm, ptL, pts, bn, bn2, Ls, ph);
+      const int stR = rside_star<T>(R, sR, sm, ptR, pts, bn, bn2, Rs, ph);
+      if (stL != HLLD_OK || stR != HLLD_OK) {
+        status = (stL != HLLD_OK) ? stL : stR;
+        break;
+      }
+      const T isqL = fast_rsqrt(Ls.rho), isqR = fast_rsqrt(Rs.rho);
+      const T sqL = Ls.rho * isqL, sqR = Rs.rho * isqR;
+      const T sgn = (bn < (T)0.0) ? (T)-1.0 : (T)1.0;
+      const T abn = vabs(bn);
+      const T sLs = sm - abn * isqL, sRs = sm + abn * isqR;
+      const T den = sqL + sqR;
+      if (den <= (T)0.0) {
+        status = HLLD_FALLBACK_DEGENERATE;
+        break;
+      }
+      const T inv = fast_rcp(den);
+      const T sq2 = sgn * sqL * sqR;
+      const T vt1D = (sqL * Ls.vt1 + sqR * Rs.vt1 + sgn * (Rs.bt1 - Ls.bt1)) * inv;
+      const T vt2D = (sqL * Ls.vt2 + sqR * Rs.vt2 + sgn * (Rs.bt2 - Ls.bt2)) * inv;
+      const T bt1D = (sqL * Rs.bt1 + sqR * Ls.bt1 + sq2 * (Rs.vt1 - Ls.vt1)) * inv;
+      const T bt2D = (sqL * Rs.bt2 + sqR * Ls.bt2 + sq2 * (Rs.vt2 - Ls.vt2)) * inv;
+      const T vbD = sm * bn + vt1D * bt1D + vt2D * bt2D;
+      const T eLD = Ls.e - sgn * sqL * (Ls.vb - vbD);
+      const T eRD = Rs.e + sgn * sqR * (Rs.vb - vbD);
+      const T v2D = sm * sm + vt1D * vt1D + vt2D * vt2D;
+      const T b2D = bn2 + bt1D * bt1D + bt2D * bt2D;
+      const T pLD = ph.gm1 * (eLD - (T)0.5 * Ls.rho * v2D - (T)0.5 * b2D);
+      const T pRD = ph.gm1 * (eRD - (T)0.5 * Rs.rho * v2D - (T)0.5 * b2D);
+      if (!(pLD > p_floor<T>() && pRD > p_floor<T>())) {
+        status = HLLD_FALLBACK_NONPHYSICAL;
+        break;
+      }
+      if (sm >= (T)0.0) {
+        rside_flux<T, AX>(L, bn, bn2, F);
+        rside_jump<T, AX>(L, Ls, sm, sL, F);
+        if (sLs < (T)0.0) rside_jump2<T, AX>(Ls, vt1D, vt2D, bt1D, bt2D, eLD, sLs, F);
+      } else {
+        rside_flux<T, AX>(R, bn, bn2, F);
+        rside_jump<T, AX>(R, Rs, sm, sR, F);
+        if (sRs >= (T)0.0) rside_jump2<T, AX>(Rs, vt1D, vt2D, bt1D, bt2D, eRD, sRs, F);
+      }
+      return HLLD_OK;
+    } while (false);
+  }
+  rside_hll<T, AX>(L, R, bn, bn2, sL, sR, F);
+  return status;
+}
+
+// GLM-augmented physical flux along AX of a face given by its primitives P
+// and total energy e (glm_phys_flux without recovering the primitives from
+// the conserved state).
+template <class T, int AX>
+PMHD_HD void glm_phys_flux_prim(const T* P, T e, T ch2, T* F) {
+  using D = Dir<AX>;
+  phys_flux<T, AX>(P, e, F);
+  F[D::bn] = P[PSI];
+  F[PSI] = ch2 * P[D::bn];
+}
+
+// state_usable with one reciprocal of the density: density and pressure
+// above the floors, all nine slots finite.
+template <class T>
+PMHD_HD bool state_usable_fast(const T* U, const Phys<T>& ph) {
+  if (!(U[RHO] > rho_floor<T>())) return false;
+  const T inv = fast_rcp(U[RHO]);
+  const T m2 = U[MX] * U[MX] + U[MY] * U[MY] + U[MZ] * U[MZ];
+  const T b2 = U[BX] * U[BX] + U[BY] * U[BY] + U[BZ] * U[BZ];
+  const T p = ph.gm1 * (U[EN] - (T)0.5 * m2 * inv - (T)0.5 * b2);
+  T sum = U[0];
+#pragma unroll
+  for (int k = 1; k < NV9; k++) sum += U[k];
+  return p > p_floor<T>() && vfinite(sum) && vfinite(p);
+}
+
+// Signal speed of one cell (cell_speed with one reciprocal of the density).
+template <class T>
+PMHD_HD T cell_speed_fast(const T* P, const Phys<T>& ph) {
+  const T inv = fast_rcp(vmax(P[RHO], rho_floor<T>()));
+  const T a2 = ph.gamma * vmax(P[EN], p_floor<T>()) * inv;
+  const T bx2 = P[BX] * P[BX], by2 = P[BY] * P[BY];
+  const T b2 = (bx2 + by2 + P[BZ] * P[BZ]) * inv;
+  const T sum = a2 + b2, s2 = sum * sum, a4 = (T)4.0 * a2 * inv;
+  const T cfx = fast_sqrt(vmax((T)0.5 * (sum + fast_sqrt(vmax(s2 - a4 * bx2, (T)0.0))), (T)0.0));
+  const T cfy = fast_sqrt(vmax((T)0.5 * (sum + fast_sqrt(vmax(s2 - a4 * by2, (T)0.0))), (T)0.0));
+  return vmax(vabs(P[MX]) + cfx, vabs(P[MY]) + cfy);
+}
+
+// Minmod as min/max selections: minmod(a, b) = max(min(a, b), min(max(a, b),
+// 0)); the same value as minmod() for finite arguments.
+template <class T>
+PMHD_HD T minmod_fast(T a, T b) {
+  return vmax(vmin(a, b), vmin(vmax(a, b), (T)0.0));
 }
 
 }  // namespace pmhd

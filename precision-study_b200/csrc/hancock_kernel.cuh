@@ -127,6 +127,21 @@ __device__ __forceinline__ void hancock_faces(HancockTileOf<Pol>& s, const Hanco
       Ps[k] = s.P[k][c - RW];
       Pn[k] = s.P[k][c + RW];
     }
+#if PMHD_FAST_FLUX
+    // Performance build: the predictor's fluxes from the face primitives
+    // (glm_phys_flux_prim), no recovery from the conserved faces.
+    const R ch2 = ch * ch;
+    recon_cell<R>(Pw, P0, Pe, Pl, Pr);
+    prim9_to_state<R>(Pl, Uf[0], ph);
+    prim9_to_state<R>(Pr, Uf[1], ph);
+    glm_phys_flux_prim<R, 0>(Pl, Uf[0][EN], ch2, F[0]);
+    glm_phys_flux_prim<R, 0>(Pr, Uf[1][EN], ch2, F[1]);
+    recon_cell<R>(Ps, P0, Pn, Pl, Pr);
+    prim9_to_state<R>(Pl, Uf[2], ph);
+    prim9_to_state<R>(Pr, Uf[3], ph);
+    glm_phys_flux_prim<R, 1>(Pl, Uf[2][EN], ch2, F[2]);
+    glm_phys_flux_prim<R, 1>(Pr, Uf[3][EN], ch2, F[3]);
+#else
     recon_cell<R>(Pw, P0, Pe, Pl, Pr);
     prim9_to_state<R>(Pl, Uf[0], ph);
     prim9_to_state<R>(Pr, Uf[1], ph);
@@ -137,6 +152,7 @@ __device__ __forceinline__ void hancock_faces(HancockTileOf<Pol>& s, const Hanco
     glm_phys_flux<R, 0>(Uf[1], ch, F[1], ph);
     glm_phys_flux<R, 1>(Uf[2], ch, F[2], ph);
     glm_phys_flux<R, 1>(Uf[3], ch, F[3], ph);
+#endif
     R corr[NVAR];
 #pragma unroll
     for (int k = 0; k < NVAR; k++) corr[k] = hx * (F[1][k] - F[0][k]) + hy * (F[3][k] - F[2][k]);
@@ -146,7 +162,7 @@ __device__ __forceinline__ void hancock_faces(HancockTileOf<Pol>& s, const Hanco
 #pragma unroll
       for (int k = 0; k < NVAR; k++) h[k] = Uf[f][k] - corr[k];
       h[PSI] = h[PSI] - hdamp * Uf[f][PSI];
-      const bool ok = state_usable<R>(h, ph);
+      const bool ok = PMHD_FAST_FLUX ? state_usable_fast<R>(h, ph) : state_usable<R>(h, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) s.H[f][k][q] = ok ? h[k] : Uf[f][k];
     }
@@ -167,6 +183,7 @@ __device__ __forceinline__ void hancock_fluxes(HancockTileOf<Pol>& s, const Memb
   constexpr int BW = HT::BW, TYH = HT::TYH;
   R* Fx = &s.f.Fx[0][0];
   R* Gy = &s.f.Gy[0][0];
+  const GlmK<R> gk = GlmK<R>::make(ch);
   for (int q = first; q < HT::NFX + HT::NGY; q += step) {
     R a[NVAR], b[NVAR], F[NVAR];
     int st;
@@ -178,7 +195,7 @@ __device__ __forceinline__ void hancock_fluxes(HancockTileOf<Pol>& s, const Memb
         a[k] = s.H[1][k][bl];
         b[k] = s.H[0][k][br];
       }
-      st = glm_flux<R, 0>(a, b, ch, HLLD, F, ph);
+      st = PMHD_FAST_FLUX ? glm_flux_fast_cons<R, 0>(a, b, gk, HLLD, F, ph) : glm_flux<R, 0>(a, b, ch, HLLD, F, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Fx[k * HT::NFX + q] = F[k];
     } else {
@@ -189,7 +206,7 @@ __device__ __forceinline__ void hancock_fluxes(HancockTileOf<Pol>& s, const Memb
         a[k] = s.H[3][k][bb];
         b[k] = s.H[2][k][bt];
       }
-      st = glm_flux<R, 1>(a, b, ch, HLLD, F, ph);
+      st = PMHD_FAST_FLUX ? glm_flux_fast_cons<R, 1>(a, b, gk, HLLD, F, ph) : glm_flux<R, 1>(a, b, ch, HLLD, F, ph);
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Gy[k * HT::NGY + g] = F[k];
     }
@@ -238,10 +255,13 @@ __device__ __forceinline__ void hancock_update(const HancockTileOf<Pol>& s, cons
     auto old = [&](int k) { return UIN_SMEM ? s.U[k][rc] : uin[(size_t)k * m.plane + g]; };
     S Un[NVAR];
     if constexpr (!Pol::kMixed) {
+      const R idx = (R)m.inv_dx, idy = (R)m.inv_dy;
 #pragma unroll
       for (int k = 0; k < NVAR; k++) {
-        R rhs = -(Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c]) / c0.dx -
-                (Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c]) / c0.dy;
+        const R dfx = Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c];
+        const R dgy = Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c];
+        // The performance build multiplies by 1 / dx, 1 / dy (Member).
+        R rhs = PMHD_FAST_FLUX ? -dfx * idx - dgy * idy : -dfx / c0.dx - dgy / c0.dy;
         const S u = old(k);
         if (k == PSI) rhs -= c0.damping * u;
         Un[k] = u + c0.dt * rhs;
@@ -249,12 +269,11 @@ __device__ __forceinline__ void hancock_update(const HancockTileOf<Pol>& s, cons
     } else {
       // Binary32 flux differences, binary64 scaling and accumulation (as
       // the mixed stage kernel).
-      const double inv_dx = 1.0 / m.dx, inv_dy = 1.0 / m.dy;
 #pragma unroll
       for (int k = 0; k < NVAR; k++) {
         const float dfx = Fx[k * HT::NFX + r * (TX + 1) + c + 1] - Fx[k * HT::NFX + r * (TX + 1) + c];
         const float dgy = Gy[k * HT::NGY + (r + 1) * TX + c] - Gy[k * HT::NGY + r * TX + c];
-        double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
+        double rhs = -(double)dfx * m.inv_dx - (double)dgy * m.inv_dy;
         const S u = old(k);
         if (k == PSI) rhs -= c0.damping * u;
         Un[k] = u + c0.dt * rhs;
@@ -271,7 +290,8 @@ __device__ __forceinline__ void hancock_update(const HancockTileOf<Pol>& s, cons
       R Pr[NVAR];
 #pragma unroll
       for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
-      const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, ph));
+      const unsigned long long b =
+          speed_bits((double)(PMHD_FAST_FLUX ? cell_speed_fast<R>(Pr, ph) : cell_speed<R>(Pr, ph)));
       sp = b > sp ? b : sp;
     }
   }

@@ -26,7 +26,10 @@ enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
 
 // Tile heights compiled into the library (tile width is 32).  Index into
 // Member::tm and the Batch tile tables; index 0 is the default.
-constexpr int kTileHeights[2] = {16, 8};
+#ifndef PMHD_TY0
+#define PMHD_TY0 19
+#endif
+constexpr int kTileHeights[2] = {PMHD_TY0, 8};
 constexpr int kNumTileHeights = 2;
 // A batched stage launch hands its CTAs runs of this many consecutive tiles.
 constexpr int kBatchRun = 16;
@@ -44,6 +47,7 @@ struct alignas(64) Member {
   int bc[4];          // x low, x high, y low, y high
   double gamma, tol;
   double cfl, alpha, dx, dy;  // exact in the precision's time type
+  double inv_dx, inv_dy;      // 1 / dx, 1 / dy divided in the precision's time type
 };
 
 // The work list of one tile height.

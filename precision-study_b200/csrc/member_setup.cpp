@@ -60,11 +60,15 @@ void set_member_physics(Member& m, double x_min, double x_max, double y_min, dou
     m.dy = (double)(((float)y_max - (float)y_min) / (float)m.ny);
     m.cfl = (double)(float)cfl;
     m.alpha = (double)(float)alpha;
+    m.inv_dx = (double)(1.0f / (float)m.dx);
+    m.inv_dy = (double)(1.0f / (float)m.dy);
   } else {
     m.dx = (x_max - x_min) / (double)m.nx;
     m.dy = (y_max - y_min) / (double)m.ny;
     m.cfl = cfl;
     m.alpha = alpha;
+    m.inv_dx = 1.0 / m.dx;
+    m.inv_dy = 1.0 / m.dy;
   }
   m.gamma = gamma;
   m.tol = tol;

@@ -108,12 +108,18 @@ constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 //         (the update reads shared memory);
 //   minb  resident CTAs per SM the register allocation is sized for.
 // 32 x 8 tiles: fp64 1 buffer / 2 CTAs (a small spill beats halving the
-// resident warps), fp32 1 / 3, mixed 2 / 2.  32 x 16 tiles (the default: 17
-// warps, one CTA per SM) recompute fewer halo interfaces and recoveries
-// (2.09 interface solves and 1.41 recoveries per cell instead of 2.16 and
-// 1.63) and run 1-4 % faster at 4096^2; 32 x 4 tiles keep about the same
-// threads per SM as 32 x 8.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64
-// override the 32 x 8 values for tuning experiments.
+// resident warps), fp32 1 / 3, mixed 2 / 2.  The default tile is 32 x 19
+// with one CTA per SM: 20 warps, five on each of the SM's four schedulers,
+// whose 16 K-register files then allow 96 registers a thread.  A 32 x 16
+// tile has 17 warps (5 / 4 / 4 / 4 per scheduler, so the same 96-register
+// cap with fewer warps), a 32 x 15 tile 16 warps at 128 registers.  At
+// 4096^2 (performance build) 32 x 19 runs mixed 5.91, fp64 2.42, fp32 6.68 G
+// zone-cycles/s against 5.25 / 2.20 / 6.04 at 32 x 16 and 5.90 / 2.28 / 6.69
+// at 32 x 15; it also recomputes the fewest halo interfaces and recoveries
+// (2.08 interface solves and 1.34 recoveries per cell; 32 x 16: 2.09 / 1.41;
+// 32 x 8: 2.16 / 1.63).  32 x 4 tiles keep about the same threads per SM as
+// 32 x 8.  PMHD_NBUF / PMHD_MINB_R32 / PMHD_MINB_R64 override the 32 x 8
+// values for tuning experiments.
 template <class Pol, int TY>
 struct Tune {
   static constexpr bool r64 = sizeof(typename Pol::R) == 8;
@@ -177,7 +183,8 @@ __device__ __forceinline__ void recover_cell(const typename Pol::S* U, typename 
                                              const Phys<typename Pol::S>& ph) {
   if constexpr (Pol::kMixed) {
     const double rho = fmax(U[RHO], 1.0e-12);
-    const double inv = 1.0 / rho;
+    // Performance build: Newton-refined reciprocal (within binary64 rounding).
+    const double inv = PMHD_FAST_FLUX ? rcp_newton(rho) : 1.0 / rho;
     const double vx = U[MX] * inv, vy = U[MY] * inv, vz = U[MZ] * inv;
     const double bx = U[BX], by = U[BY], bz = U[BZ];
     const double v2 = vx * vx + vy * vy + vz * vz;
@@ -187,6 +194,22 @@ __device__ __forceinline__ void recover_cell(const typename Pol::S* U, typename 
     P[MY] = vy;
     P[MZ] = vz;
     P[EN] = ph.gm1 * (U[EN] - 0.5 * rho * v2 - 0.5 * b2);
+    P[BX] = bx;
+    P[BY] = by;
+    P[BZ] = bz;
+    P[PSI] = U[PSI];
+  } else if (PMHD_FAST_FLUX) {
+    // Performance build: one reciprocal of the density for the velocities.
+    using S = typename Pol::S;
+    const S rho = vmax(U[RHO], rho_floor<S>());
+    const S inv = fast_rcp(rho);
+    const S vx = U[MX] * inv, vy = U[MY] * inv, vz = U[MZ] * inv;
+    const S bx = U[BX], by = U[BY], bz = U[BZ];
+    P[RHO] = rho;
+    P[MX] = vx;
+    P[MY] = vy;
+    P[MZ] = vz;
+    P[EN] = ph.gm1 * (U[EN] - (S)0.5 * rho * (vx * vx + vy * vy + vz * vz) - (S)0.5 * (bx * bx + by * by + bz * bz));
     P[BX] = bx;
     P[BY] = by;
     P[BZ] = bz;
@@ -270,7 +293,7 @@ __device__ __forceinline__ void store_cell(S* u, long long plane, int pitch, int
 //          in tiles with an unusable cell, see cell_usable_fast)
 template <class Pol, bool HLLD, int TC>
 __device__ __forceinline__ int face_flux(const typename Pol::R* sP, bool checks, int base, int stride, int o1,
-                                         int o2, int o5, int o6, int muscl, typename Pol::R ch,
+                                         int o2, int o5, int o6, int muscl, const GlmK<typename Pol::R>& gk,
                                          const Phys<typename Pol::R>& ph, typename Pol::R* F) {
   using R = typename Pol::R;
   const int off[NVAR] = {0, o1, o2, 3 * TC, 4 * TC, o5, o6, 7 * TC, 8 * TC};
@@ -289,23 +312,23 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, bool checks,
     if (PMHD_FAST_FLUX && !checks) {
 #pragma unroll
       for (int k = 0; k < NVAR; k++) {
-        Pa[k] = P0[k] + (R)0.5 * minmod(P0[k] - Pm[k], P1[k] - P0[k]);
-        Pb[k] = P1[k] - (R)0.5 * minmod(P1[k] - P0[k], P2[k] - P1[k]);
+        const R d1 = P1[k] - P0[k];
+        Pa[k] = P0[k] + (R)0.5 * minmod_fast(P0[k] - Pm[k], d1);
+        Pb[k] = P1[k] - (R)0.5 * minmod_fast(d1, P2[k] - P1[k]);
       }
     } else {
       R Pl[NVAR];
       recon_cell<R>(Pm, P0, P1, Pl, Pa);
       recon_cell<R>(P0, P1, P2, Pb, Pl);
     }
-    if (PMHD_FAST_FLUX && sizeof(R) == 8) {
-      // Performance build, fp64: the face primitives go to the solver
-      // directly instead of a primitive -> conserved -> primitive trip.
-      // (The fp32-flux policies keep the trip: their register budgets would
-      // spill.)
-      return glm_flux_prim<R, 0>(Pa, Pb, ch, HLLD, F, ph);
-    }
+#if PMHD_FAST_FLUX
+    // Performance build: the face primitives go to the solver directly
+    // (glm_flux_fast), no primitive -> conserved -> primitive trip.
+    return glm_flux_fast<R, 0>(Pa, Pb, gk, HLLD, F, ph);
+#else
     prim9_to_state<R>(Pa, UL, ph);
     prim9_to_state<R>(Pb, UR, ph);
+#endif
   } else {  // first order: sP holds the conserved states
 #pragma unroll
     for (int k = 0; k < NVAR; k++) {
@@ -313,7 +336,7 @@ __device__ __forceinline__ int face_flux(const typename Pol::R* sP, bool checks,
       UR[k] = sP[off[k] + base + 2 * stride];
     }
   }
-  return glm_flux<R, 0, PMHD_FAST_FLUX != 0>(UL, UR, ch, HLLD, F, ph);
+  return glm_flux<R, 0, PMHD_FAST_FLUX != 0>(UL, UR, gk.ch, HLLD, F, ph);
 }
 
 // Per-member step values (uniform for all tiles of a member in one launch).
@@ -582,7 +605,7 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
       const int o1 = (axis ? 2 : 1) * TC, o2 = (axis ? 1 : 2) * TC;
       const int o5 = (axis ? 6 : 5) * TC, o6 = (axis ? 5 : 6) * TC;
       R F[NVAR];
-      const int st = face_flux<Pol, HLLD, TC>(sP, checks, base, stride, o1, o2, o5, o6, m.muscl, v.ch, phR, F);
+      const int st = face_flux<Pol, HLLD, TC>(sP, checks, base, stride, o1, o2, o5, o6, m.muscl, GlmK<R>::make(v.ch), phR, F);
       R* out = axis ? sGy : sFx;
       const int n_out = axis ? GYN : FXN;
       const int item = axis ? fy * TX + fx : fy * (TX + 1) + fx;
@@ -613,14 +636,18 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
       S* u_out = static_cast<S*>(STAGE == 1 ? m.u1 : m.u);
       S Un[NVAR];
       if constexpr (!Pol::kMixed) {
-        // Reference order (mhd2d_glm_gpu.cu:282-285, :299, :316-317).
+        // Reference order (mhd2d_glm_gpu.cu:282-285, :299, :316-317); the
+        // performance build multiplies by 1 / dx, 1 / dy (Member) instead of
+        // dividing.
         const R damping = v.ch / vmax((R)m.alpha, (R)1.0e-12);
         const R dxR = (R)m.dx, dyR = (R)m.dy, dtR = (R)v.dt;
+        const R idxR = (R)m.inv_dx, idyR = (R)m.inv_dy;
 #pragma unroll
         for (int k = 0; k < NVAR; k++) {
           const R uin = NBUF == 2 ? sU[k * TC + lc] : u_in[(size_t)k * m.plane + gidx];
-          R rhs = -(sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx]) / dxR -
-                  (sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx]) / dyR;
+          const R dfx = sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx];
+          const R dgy = sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx];
+          R rhs = PMHD_FAST_FLUX ? -dfx * idxR - dgy * idyR : -dfx / dxR - dgy / dyR;
           if (k == PSI) rhs -= damping * uin;
           if (STAGE == 1) {
             Un[k] = uin + dtR * rhs;
@@ -631,15 +658,14 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
         }
       } else {
         // Binary32 fluxes and their differences, binary64 scaling and
-        // accumulation.
+        // accumulation (m.inv_dx = 1.0 / dx in binary64, set on the host).
         const double damping = (double)v.ch / fmax(m.alpha, 1.0e-12);
-        const double inv_dx = 1.0 / m.dx, inv_dy = 1.0 / m.dy;
 #pragma unroll
         for (int k = 0; k < NVAR; k++) {
           const double uin = NBUF == 2 ? sU[k * TC + lc] : u_in[(size_t)k * m.plane + gidx];
           const float dfx = sFx[k * FXN + ty * (TX + 1) + tx + 1] - sFx[k * FXN + ty * (TX + 1) + tx];
           const float dgy = sGy[k * GYN + (ty + 1) * TX + tx] - sGy[k * GYN + ty * TX + tx];
-          double rhs = -(double)dfx * inv_dx - (double)dgy * inv_dy;
+          double rhs = -(double)dfx * m.inv_dx - (double)dgy * m.inv_dy;
           if (k == PSI) rhs -= damping * uin;
           if (STAGE == 1) {
             Un[k] = uin + (double)v.dt * rhs;
@@ -662,7 +688,8 @@ __global__ void __launch_bounds__(Geo<TY>::NT, Tune<Pol, TY>::minb)
         R Pr[NVAR];
 #pragma unroll
         for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
-        const unsigned long long sb = speed_bits((double)cell_speed<R>(Pr, phR));
+        const unsigned long long sb =
+            speed_bits((double)(PMHD_FAST_FLUX ? cell_speed_fast<R>(Pr, phR) : cell_speed<R>(Pr, phR)));
         acc.sp_bits = sb > acc.sp_bits ? sb : acc.sp_bits;
       }
     }
@@ -692,7 +719,8 @@ __global__ void __launch_bounds__(NTA) speed_kernel(const typename Pol::S* __res
     recover_cell<Pol>(U9, P9, phS);
 #pragma unroll
     for (int k = 0; k < NVAR; k++) Pr[k] = (R)P9[k];
-    const unsigned long long b = speed_bits((double)cell_speed<R>(Pr, phR));
+    const unsigned long long b =
+        speed_bits((double)(PMHD_FAST_FLUX ? cell_speed_fast<R>(Pr, phR) : cell_speed<R>(Pr, phR)));
     m = b > m ? b : m;
   }
   __shared__ unsigned long long red[NTA / 32];
