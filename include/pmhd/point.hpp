@@ -669,7 +669,7 @@ struct GlmK {
     GlmK k;
     k.ch = c;
     k.ch_safe = vmax(c, (T)1.0e-12);
-    k.half_inv = (T)0.5 / k.ch_safe;
+    k.half_inv = (T)0.5 * fast_rcp(k.ch_safe);
     k.ch2 = c * c;
     return k;
   }
