@@ -513,9 +513,14 @@ def bench_ensemble(pmhd, nmem, seed, prec, W, K, device, barrier, max_over_ranks
     barrier()
     ms = max_over_ranks(tot.device_ms)
     cells = sum(m.nx * m.ny for m in ms_desc)
+    # Tile height each size class runs with (the autotuner times each class).
+    heights = {}
+    for k, d in enumerate(ms_desc):
+        heights.setdefault(str(d.nx), e.member_stats(k).tile_height)
     out = {"value": world * tot.zone_cycles / (ms / 1e3), "unit": UNIT, "members": nmem, "seed": seed,
            "cells": cells, "steps": K, "warmup_steps": max(32, W), "ms_per_step": ms / K,
-           "tile_height": tot.tile_height, "ctas": tot.ctas, "gpu_launches": tot.kernel_launches,
+           "tile_height": tot.tile_height, "tile_height_by_size": heights, "ctas": tot.ctas,
+           "gpu_launches": tot.kernel_launches,
            "status": tot.status,
            "sizes": {str(s): sum(1 for m in ms_desc if m.nx == s) for s in (64, 128, 256, 512)}}
     e.close()

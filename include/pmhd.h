@@ -94,10 +94,11 @@ typedef struct {
   int steps_per_graph;              /* steps captured per CUDA graph, 0 = auto */
   int autotune;                     /* 1: the first pmhd_advance that runs at least
                                        32 steps times every stage-kernel variant
-                                       (32x16 / 32x8 tiles x resident CTAs per SM)
-                                       on 2 live steps each and keeps the fastest;
+                                       (32x19 / 32x8 tiles x resident CTAs per SM)
+                                       on 2 live steps each and keeps the fastest
+                                       (an ensemble: per grid size, see below);
                                        results do not depend on the variant.
-                                       0: 32x16 tiles, all resident CTAs.      */
+                                       0: 32x19 tiles, all resident CTAs.      */
 } pmhd_config;
 
 typedef struct {
@@ -203,7 +204,10 @@ int pmhd_get_config(const pmhd_solver* s, pmhd_config* cfg);
  * member has its own grid size, domain, gamma, boundary kinds, initial
  * condition and end time, and advances with its own CFL time step; all
  * members' tiles form one work list of one persistent stage launch per SSPRK2
- * stage, replayed from CUDA graphs.  The common configuration supplies
+ * stage, replayed from CUDA graphs.  With autotune, every grid size is timed
+ * on its own and the sizes that choose the same tile height share one work
+ * list: a stage is then one launch per chosen tile height.  The common
+ * configuration supplies
  * precision, exact, order, solver, cfl, alpha, hlld_tol, device,
  * steps_per_graph and autotune (its nx, ny, domain, gamma and bc are
  * ignored).  Each member gives the same results as a single pmhd_solver run

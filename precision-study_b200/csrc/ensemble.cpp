@@ -46,6 +46,8 @@ struct pmhd_ensemble {
   std::vector<long long> steps;
   std::vector<char> failed;        // member halted on an unusable cell
   bool broken = false;             // a CUDA error or device timeout
+  std::vector<int> member_ty;      // tile-height index each member runs with
+  std::vector<int*> plan_lists;    // device work lists of the per-size plan
 };
 
 namespace {
@@ -125,6 +127,140 @@ double time_type(const pmhd_ensemble* e, double v) {
   return e->cfg.precision == PMHD_FP32 ? (double)(float)v : v;
 }
 
+// Work list (tile -> member, member -> first tile) of the members `ms` at
+// tile height index t, copied to new device arrays.
+cudaError_t make_work_list(pmhd_ensemble* e, const std::vector<int>& ms, int t, Batch* b, int** d_tiles,
+                           int** d_tile0) {
+  const int n = (int)e->desc.size();
+  std::vector<int> tiles, tile0(n, 0);
+  for (int k : ms) {
+    tile0[k] = (int)tiles.size();
+    const long long nt = (long long)((e->desc[k].nx + 31) / 32) *
+                         ((e->desc[k].ny + kTileHeights[t] - 1) / kTileHeights[t]);
+    tiles.insert(tiles.end(), (size_t)nt, k);
+  }
+  *d_tiles = nullptr;
+  *d_tile0 = nullptr;
+  cudaError_t err = cudaMalloc(d_tiles, sizeof(int) * tiles.size());
+  if (err == cudaSuccess) err = cudaMalloc(d_tile0, sizeof(int) * n);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(*d_tiles, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, e->stream);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(*d_tile0, tile0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+  b->members = e->dMembers;
+  b->tile_member = *d_tiles;
+  b->member_tile0 = *d_tile0;
+  b->nmembers = n;
+  b->ntiles = (int)tiles.size();
+  return err;
+}
+
+// The autotuner of an ensemble: every size class (members of one grid size)
+// is timed on its own -- two live steps of only that class's members per
+// kernel variant (tile height x resident CTAs per SM); the variants compute
+// identical results, so these are ordinary steps of those members -- and
+// keeps its fastest variant.  The classes that chose the same tile height
+// then share one work list, whose CTA count is that of its largest class by
+// cells; a step launches each such part's stage 1, then each part's stage 2.
+// Returns the fewest tuning steps any member took (for step budgets) and
+// adds the launches made to *launched.
+cudaError_t tune_by_size(pmhd_ensemble* e, long long* min_steps, long long* launched) {
+  const int n = (int)e->desc.size();
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  std::vector<std::pair<int, int>> keys;
+  std::vector<std::vector<int>> classes;
+  for (int k = 0; k < n; k++) {
+    const std::pair<int, int> key(e->desc[k].nx, e->desc[k].ny);
+    size_t c = 0;
+    while (c < keys.size() && keys[c] != key) c++;
+    if (c == keys.size()) {
+      keys.push_back(key);
+      classes.emplace_back();
+    }
+    classes[c].push_back(k);
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  std::vector<LaunchPart> best(classes.size());
+  cudaError_t err = cudaSuccess;
+  *min_steps = -1;
+  for (size_t c = 0; c < classes.size() && err == cudaSuccess; c++) {
+    float best_ms = -1.f;
+    long long steps = 0;
+    for (int t = 0; t < kNumTileHeights && err == cudaSuccess; t++) {
+      LaunchPart part;
+      part.ty_idx = t;
+      int *dt = nullptr, *d0 = nullptr;
+      err = make_work_list(e, classes[c], t, &part.batch, &dt, &d0);
+      const int occ = e->kt->ctas_per_sm(e->cfg.precision, e->run.hlld, t, 1);
+      for (int k = occ; k >= 1 && err == cudaSuccess; k--) {
+        part.grid = k == occ ? 0 : sms * k;
+        e->run.set_parts(std::vector<LaunchPart>(1, part));
+        cudaEventRecord(e0, e->stream);
+        err = e->run.enqueue_steps(2);
+        cudaEventRecord(e1, e->stream);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        steps += 2;
+        *launched += 4;
+        if (best_ms < 0.f || ms < best_ms) {
+          best_ms = ms;
+          best[c] = part;
+        }
+      }
+      cudaStreamSynchronize(e->stream);
+      if (dt) cudaFree(dt);
+      if (d0) cudaFree(d0);
+    }
+    if (*min_steps < 0 || steps < *min_steps) *min_steps = steps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) {
+    e->run.set_parts(std::vector<LaunchPart>());
+    return err;
+  }
+  // One part per chosen tile height.
+  std::vector<LaunchPart> parts;
+  for (int t = 0; t < kNumTileHeights && err == cudaSuccess; t++) {
+    std::vector<int> ms;
+    long long top_cells = -1;
+    int grid = 0;
+    for (size_t c = 0; c < classes.size(); c++) {
+      if (best[c].ty_idx != t) continue;
+      const long long cells = (long long)keys[c].first * keys[c].second * (long long)classes[c].size();
+      if (cells > top_cells) {
+        top_cells = cells;
+        grid = best[c].grid;
+      }
+    }
+    for (int k = 0; k < n; k++) {
+      size_t c = 0;
+      while (keys[c] != std::pair<int, int>(e->desc[k].nx, e->desc[k].ny)) c++;
+      if (best[c].ty_idx == t) {
+        ms.push_back(k);
+        e->member_ty[k] = t;
+      }
+    }
+    if (ms.empty()) continue;
+    LaunchPart part;
+    part.ty_idx = t;
+    part.grid = grid;
+    int *dt = nullptr, *d0 = nullptr;
+    err = make_work_list(e, ms, t, &part.batch, &dt, &d0);
+    if (dt) e->plan_lists.push_back(dt);
+    if (d0) e->plan_lists.push_back(d0);
+    parts.push_back(part);
+  }
+  e->run.set_parts(err == cudaSuccess ? parts : std::vector<LaunchPart>());
+  return err;
+}
+
 bool finished(const Ctrl& c) { return !(c.t[0] < c.t_end) || c.step[0] >= c.step_limit; }
 bool failing(const Ctrl& c) { return c.halted || c.bad1 != BAD_NONE || c.bad2 != BAD_NONE; }
 
@@ -175,6 +311,7 @@ int pmhd_ensemble_destroy(pmhd_ensemble* e) {
   cudaSetDevice(e->cfg.device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   e->run.release();
+  for (int* d : e->plan_lists) cudaFree(d);
   for (int t = 0; t < kNumTileHeights; t++) {
     if (e->dTiles[t]) cudaFree(e->dTiles[t]);
     if (e->dTile0[t]) cudaFree(e->dTile0[t]);
@@ -224,6 +361,7 @@ int pmhd_ensemble_create(const pmhd_config* common, const pmhd_member_desc* memb
   e->t.assign(n, 0.0);
   e->steps.assign(n, 0);
   e->failed.assign(n, 0);
+  e->member_ty.assign(n, 0);
   int rc = PMHD_OK;
   if (e->kt->init() != cudaSuccess) rc = PMHD_ERR_CUDA;
   // Layout of the member states.
@@ -361,14 +499,12 @@ int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* tot
   }
   long long tune_steps = 0, launched = n;  // kernels enqueued: n CFL reductions so far
   if (e->cfg.autotune && !e->tuned && (max_steps < 0 || max_steps >= 32)) {
-    // Live steps timed per kernel variant; identical results for every variant.
-    TuneResult tr;
-    PMHD_E(e->run.tune(2, &tr));
-    tune_steps = 2LL * tr.candidates;
-    launched += 2 * tune_steps;
+    // Live steps timed per size class and kernel variant (tune_by_size).
+    PMHD_E(tune_by_size(e, &tune_steps, &launched));
     e->tuned = true;
   }
   const int big = e->cfg.steps_per_graph;
+  const long long per_step = 2LL * (e->run.parts.empty() ? 1 : (long long)e->run.parts.size());
   // Done when every member has finished or failed, or on a device timeout.
   auto all_done = [n](const Ctrl* cs) {
     for (int k = 0; k < n; k++)
@@ -385,8 +521,8 @@ int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* tot
     cudaGraphExec_t gb = nullptr, g2 = nullptr;
     if (left >= big && e->run.graph(big, &gb) != 0) return PMHD_ERR_CUDA;
     if (e->run.graph(2, &g2) != 0) return PMHD_ERR_CUDA;
-    for (; left >= big; left -= big, launched += 2LL * big) PMHD_E(cudaGraphLaunch(gb, e->stream));
-    for (; left > 0; left -= 2, launched += 4) PMHD_E(cudaGraphLaunch(g2, e->stream));
+    for (; left >= big; left -= big, launched += per_step * big) PMHD_E(cudaGraphLaunch(gb, e->stream));
+    for (; left > 0; left -= 2, launched += 2 * per_step) PMHD_E(cudaGraphLaunch(g2, e->stream));
   } else {
     // Time-limited: replay graphs, polling the control blocks one replay
     // behind so the device never idles waiting for the host.
@@ -401,7 +537,7 @@ int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* tot
                               e->stream);
       if (err == cudaSuccess) err = cudaEventRecord(e->evPoll[b], e->stream);
       issued++;
-      launched += 2LL * big;
+      launched += per_step * big;
       return err;
     };
     PMHD_E(issue());
@@ -459,7 +595,7 @@ int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* tot
     if (mst != PMHD_OK || !e->failed[k]) st.status = mst;
     st.zone_cycles = (unsigned long long)done * (unsigned long long)d.nx * d.ny;
     st.device_ms = ms;
-    st.tile_height = kTileHeights[e->run.choice.ty_idx];
+    st.tile_height = kTileHeights[e->run.parts.empty() ? e->run.choice.ty_idx : e->member_ty[k]];
     if (mst != PMHD_OK && status == PMHD_OK) {
       status = mst;
       tot.bad_i = st.bad_i;
@@ -477,13 +613,26 @@ int pmhd_ensemble_advance(pmhd_ensemble* e, long long max_steps, pmhd_stats* tot
   tot.kernel_launches = (unsigned long long)launched;
   tot.status = status;
   tot.device_ms = ms;
-  tot.tile_height = kTileHeights[e->run.choice.ty_idx];
   {
+    // The launch plan's largest part (by tiles) stands for the ensemble's
+    // tile height and CTA count; each member reports its own tile height.
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->cfg.device);
-    const int def = sms * e->kt->ctas_per_sm(e->cfg.precision, e->run.hlld, e->run.choice.ty_idx, 1);
-    const int g = e->run.choice.grid > 0 ? e->run.choice.grid : def;
-    const int nt = e->run.batch[e->run.choice.ty_idx].ntiles;
+    std::vector<LaunchPart> plan = e->run.parts;
+    if (plan.empty()) {
+      LaunchPart one;
+      one.ty_idx = e->run.choice.ty_idx;
+      one.grid = e->run.choice.grid;
+      one.batch = e->run.batch[one.ty_idx];
+      plan.push_back(one);
+    }
+    size_t top = 0;
+    for (size_t q = 1; q < plan.size(); q++)
+      if (plan[q].batch.ntiles > plan[top].batch.ntiles) top = q;
+    const int def = sms * e->kt->ctas_per_sm(e->cfg.precision, e->run.hlld, plan[top].ty_idx, 1);
+    const int g = plan[top].grid > 0 ? plan[top].grid : def;
+    const int nt = plan[top].batch.ntiles;
+    tot.tile_height = kTileHeights[plan[top].ty_idx];
     tot.ctas = g < nt ? g : nt;
   }
   for (int k = 0; k < n; k++) e->mstats[k].ctas = tot.ctas;

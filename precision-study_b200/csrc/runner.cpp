@@ -13,6 +13,10 @@ cudaError_t Runner::enqueue_steps(int nsteps) const {
       if (!single) return cudaErrorNotSupported;
       e = kt->hancock(precision, hlld, 0, *single, p, stream);
       if (e == cudaSuccess) e = kt->hancock(precision, hlld, 1, *single, p, stream);
+    } else if (!parts.empty()) {
+      for (int st = 1; st <= 2 && e == cudaSuccess; st++)
+        for (size_t q = 0; q < parts.size() && e == cudaSuccess; q++)
+          e = kt->stage(precision, hlld, st, parts[q].ty_idx, parts[q].batch, single, p, parts[q].grid, stream);
     } else {
       e = kt->stage(precision, hlld, 1, choice.ty_idx, b, single, p, choice.grid, stream);
       if (e == cudaSuccess) e = kt->stage(precision, hlld, 2, choice.ty_idx, b, single, p, choice.grid, stream);
@@ -27,8 +31,9 @@ cudaError_t Runner::enqueue_steps(int nsteps) const {
 }
 
 int Runner::graph(int nsteps, cudaGraphExec_t* out) {
+  const int plan = parts.empty() ? -1 : plan_id_;
   for (auto& g : graphs_)
-    if (g.steps == nsteps && g.ty_idx == choice.ty_idx && g.grid == choice.grid) {
+    if (g.steps == nsteps && g.ty_idx == choice.ty_idx && g.grid == choice.grid && g.plan == plan) {
       *out = g.exec;
       return 0;
     }
@@ -40,7 +45,7 @@ int Runner::graph(int nsteps, cudaGraphExec_t* out) {
     if (graph) cudaGraphDestroy(graph);
     return -1;
   }
-  Graph g{nsteps, choice.ty_idx, choice.grid, nullptr};
+  Graph g{nsteps, choice.ty_idx, choice.grid, plan, nullptr};
   e = cudaGraphInstantiate(&g.exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return -1;

@@ -26,6 +26,14 @@ struct TuneResult {
   float default_ms_per_step = 0.f;  // the untuned choice (32 x 8, full occupancy)
 };
 
+// One work list of a multi-part launch plan (an ensemble whose size classes
+// run different tile heights): its tile height, persistent CTAs and tiles.
+struct LaunchPart {
+  int ty_idx = 0;
+  int grid = 0;  // 0 = SM count x resident CTAs
+  Batch batch;
+};
+
 class Runner {
  public:
   const KernelTable* kt = nullptr;
@@ -35,6 +43,14 @@ class Runner {
   Batch batch[kNumTileHeights];
   const Member* single = nullptr;  // host copy of a one-grid batch's member, or nullptr
   LaunchChoice choice;
+  // Multi-part plan: when non-empty, a step launches stage 1 of every part,
+  // then stage 2 of every part (parts hold disjoint members), instead of one
+  // launch per stage with `choice`.  Change it through set_parts().
+  std::vector<LaunchPart> parts;
+  void set_parts(const std::vector<LaunchPart>& p) {
+    parts = p;
+    plan_id_++;
+  }
   int hancock = 0;  // MUSCL-Hancock steps (single grid) instead of SSPRK2 stages
   // Optional work enqueued before and after every step (argument: the
   // step's parity), captured into the graphs with the stage launches.
@@ -53,10 +69,11 @@ class Runner {
 
  private:
   struct Graph {
-    int steps, ty_idx, grid;
+    int steps, ty_idx, grid, plan;
     cudaGraphExec_t exec;
   };
   std::vector<Graph> graphs_;
+  int plan_id_ = 0;
 };
 
 }  // namespace pmhd

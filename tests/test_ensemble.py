@@ -319,3 +319,30 @@ def test_default_ensemble_with_autotuner_matches_single_runs(pmhd_lib):
             U, st = _single(pmhd_lib, d, **common)
             assert abs(e.member_stats(k).steps - st.steps) <= 1
             _same(e.get_state(k), U, common, f"member {k}")
+
+
+@pytest.mark.gpu
+def test_per_size_tuned_plan_is_bit_identical(pmhd_lib):
+    """With autotune, each grid size is timed on its own and the sizes that
+    choose the same tile height share a work list (one launch per chosen
+    height and stage).  Whatever plan results, the exact build still gives
+    every member the bits of its single-grid run, including members that
+    took tuning steps while the others did not, and each member reports the
+    tile height of its part."""
+    m = pmhd_lib.member
+    members = [m(64, 64, t_end=0.05), m(160, 160, t_end=0.03), m(64, 64, params=(1.2,), t_end=0.05),
+               m(96, 40, problem=pmhd_lib.PROBLEM_BRIO_WU_TORUS, params=(1, 1), gamma=2.0, t_end=0.02),
+               m(160, 160, params=(0.8,), t_end=0.03)]
+    common = dict(precision="mixed", exact=True)
+    with pmhd_lib.Ensemble(members, autotune=True, **common) as e:
+        tot = e.advance()
+        assert tot.status == pmhd_lib.OK
+        heights = [e.member_stats(k).tile_height for k in range(len(members))]
+        assert set(heights) <= {19, 8}
+        assert heights[0] == heights[2] and heights[1] == heights[4]  # per size class
+        for k, d in enumerate(members):
+            U, st = _single(pmhd_lib, d, **common)
+            ms = e.member_stats(k)
+            assert ms.steps == st.steps and ms.t == st.t, k
+            assert (ms.degenerate, ms.nonphysical) == (st.degenerate, st.nonphysical), k
+            np.testing.assert_array_equal(e.get_state(k), U, err_msg=f"member {k}")
