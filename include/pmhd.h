@@ -136,6 +136,7 @@ int pmhd_destroy(pmhd_solver* s);
 /* Builds problem `problem` on the host and uploads it; resets t and the
  * step count to 0.  params may be NULL (defaults) or point to:
  *   ORSZAG_TANG:   params[0] = field amplitude factor B0 (1 = reference)
+ *   KH_REF:        params[0] = shear-layer width (the reference's 0.025)
  *   KH_REFLECT:    params[0] = shear-layer width (0.05), params[1] = Bx (0.1)
  *   BRIO_WU_2D:    params[0] = interface angle in radians (0)
  *   BRIO_WU_TORUS: params[0] = k, params[1] = m (integers >= 0, not both 0;
@@ -274,16 +275,31 @@ int pmhd_conv3x3(int mode, const void* x, int batch, int h, int w, int c_in, con
 int pmhd_conv3x3_wgrad(const void* x, const void* dz, int batch, int h, int w, int c_in, int c_out, float* dweight,
                        float* dbias, void* stream);
 
+/* Training loss of the correction network and its gradient with respect to
+ * the network output, over `batch` periodic h x w images; device pointers:
+ * out and tgt [batch][h][w][16] fp32, dz [batch][h][w][16] bf16 (16-byte
+ * aligned).  Channels 0-4, 6, 7 are compared directly with tgt; channel 5 is
+ * a potential A whose central-difference curl, dBx = cy (A(y+1) - A(y-1)),
+ * dBy = -cx (A(x+1) - A(x-1)), is compared with tgt channels 8 and 9:
+ * loss = sum of the nine squared differences / (9 batch h w).  *loss (host)
+ * receives the loss.  Synchronises `stream` before returning. */
+int pmhd_learned_loss_grad(const float* out, const float* tgt, int batch, int h, int w, float cx, float cy, void* dz,
+                           double* loss, void* stream);
+
 /* ---- Learned coarse-grid correction -------------------------------------------
  * No counterpart in the reference.  A periodic problem runs on a coarse grid
- * (nx x ny) with the plain solver; after every step a small network (three
+ * (nx x ny) with the plain solver; after every step a small network (four
  * 3x3 convolutions, 32 channels, GELU; BF16 tensor-core kernels with fp32
  * accumulation) predicts the difference between the fine solution (refine x
  * finer, restricted by block averages) and the coarse step, from the coarse
- * state and its step increment.  The correction is applied only when the
- * corrected state keeps positive density and pressure and its ||div B||_1
- * grows by at most div_tol relative to the uncorrected step; otherwise the
- * plain coarse step stands (counted as a rejection).  Training pairs come
+ * state and its step increment, in quantities that keep the corrected state
+ * physical: log ratios of density and pressure, velocity increments, and a
+ * potential whose central-difference curl corrects B_x and B_y (so the
+ * central-difference div B does not change).  The correction is applied only
+ * when the corrected state keeps positive density and pressure and its
+ * ||div B||_1 grows by at most div_tol relative to the uncorrected step;
+ * otherwise the plain coarse step stands (counted as a rejection).  Training
+ * pairs come
  * from the solver itself (pmhd_learned_generate: fine and coarse runs of a
  * problem); training runs on the device with the project's own forward and
  * backward kernels and Adam.  All four boundaries are periodic; states are
@@ -333,7 +349,8 @@ int pmhd_learned_num_pairs(const pmhd_learned* L);
 
 /* `iters` Adam steps (cosine decay from lr) on minibatches of `batch` pairs
  * drawn uniformly; losses (may be NULL, `iters` floats) receives the
- * minibatch mean squared error of the normalised correction per step.  The
+ * minibatch loss (see pmhd_learned_loss_grad; targets normalised by their
+ * root mean square) per step.  The
  * input/output normalisation is fixed from the pairs at the first call. */
 int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* losses);
 

@@ -86,8 +86,8 @@ def conv3x3_backward_weight(x, dz):
 
 
 def net_forward(x, params):
-    """Three-layer network: conv-GELU, conv-GELU, conv (linear).  params is a
-    list of (W, b) per layer.  Returns (output, cache)."""
+    """Network of len(params) layers: conv-GELU ..., then conv (linear).
+    params is a list of (W, b) per layer.  Returns (output, cache)."""
     cache = []
     a = np.asarray(x, dtype=np.float64)
     for i, (W, b) in enumerate(params):
@@ -106,6 +106,47 @@ def net_loss_and_grads(x, params, target, nvar):
     diff[..., :nvar] = out[..., :nvar] - np.asarray(target, dtype=np.float64)[..., :nvar]
     loss = float((diff ** 2).sum() / n)
     dz = 2.0 * diff / n
+    grads = [None] * len(params)
+    for i in range(len(params) - 1, -1, -1):
+        a_in, _ = cache[i]
+        grads[i] = conv3x3_backward_weight(a_in, dz)
+        if i > 0:
+            da = conv3x3_backward_input(dz, params[i][0])
+            dz = da * gelu_grad(cache[i - 1][1])
+    return loss, grads
+
+
+DIRECT = [0, 1, 2, 3, 4, 6, 7]  # channels compared directly with the target
+CH_A, CH_BX, CH_BY = 5, 8, 9     # potential; target field change
+
+
+def curl_loss_and_grad(out, target, cx, cy):
+    """Training loss of the correction network (the kernels' loss_grad):
+    squared differences of the direct channels, plus the field change
+    (target channels 8, 9) against the central-difference curl of the
+    potential in channel 5, dBx = cy (A(y+1) - A(y-1)), dBy = -cx (A(x+1) -
+    A(x-1)), periodic; divided by 9 x pixels.  Returns (loss, d loss / d out)
+    for NHWC arrays of 16 channels."""
+    out = np.asarray(out, dtype=np.float64)
+    target = np.asarray(target, dtype=np.float64)
+    n = 9 * out.shape[0] * out.shape[1] * out.shape[2]
+    d = np.zeros_like(out)
+    d[..., DIRECT] = out[..., DIRECT] - target[..., DIRECT]
+    A = out[..., CH_A]
+    rx = cy * (np.roll(A, -1, axis=1) - np.roll(A, 1, axis=1)) - target[..., CH_BX]
+    ry = -cx * (np.roll(A, -1, axis=2) - np.roll(A, 1, axis=2)) - target[..., CH_BY]
+    loss = float(((d ** 2).sum() + (rx ** 2).sum() + (ry ** 2).sum()) / n)
+    g = 2.0 * d / n
+    g[..., CH_A] = 2.0 / n * (cy * (np.roll(rx, 1, axis=1) - np.roll(rx, -1, axis=1)) +
+                              cx * (np.roll(ry, -1, axis=2) - np.roll(ry, 1, axis=2)))
+    return loss, g
+
+
+def net_curl_loss_and_grads(x, params, target, cx, cy):
+    """curl_loss_and_grad of the network output and its gradients with
+    respect to every (W, b)."""
+    out, cache = net_forward(x, params)
+    loss, dz = curl_loss_and_grad(out, target, cx, cy)
     grads = [None] * len(params)
     for i in range(len(params) - 1, -1, -1):
         a_in, _ = cache[i]

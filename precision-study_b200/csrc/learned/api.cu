@@ -1,10 +1,12 @@
-// api.cu -- C ABI of the convolution building blocks (pmhd_conv3x3,
-// pmhd_conv3x3_wgrad; declared in include/pmhd.h).
+// api.cu -- C ABI of the learned correction's building blocks
+// (pmhd_conv3x3, pmhd_conv3x3_wgrad, pmhd_learned_loss_grad; declared in
+// include/pmhd.h).
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
 #include "learned/conv.h"
+#include "learned/net.h"
 #include "pmhd.h"
 
 namespace {
@@ -75,6 +77,39 @@ int pmhd_conv3x3_wgrad(const void* x, const void* dz, int batch, int h, int w, i
                                                      static_cast<const __nv_bfloat16*>(dz), batch, h, w, c_in, c_out,
                                                      dweight, dbias, err, s);
   return finish(e, err, s);
+}
+
+int pmhd_learned_loss_grad(const float* out, const float* tgt, int batch, int h, int w, float cx, float cy, void* dz,
+                           double* loss, void* stream) {
+  if (batch < 1 || h < 1 || w < 1 || (long long)batch * h * w > (1LL << 31)) return PMHD_ERR_ARG;
+  if (!out || !tgt || !dz || !loss || !aligned16(dz)) return PMHD_ERR_ARG;
+  using namespace pmhd::learned;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Norm hn{};
+  hn.cx = cx;
+  hn.cy = cy;
+  Norm* dn = nullptr;
+  float* hist = nullptr;
+  int* it = nullptr;
+  cudaError_t e = cudaMalloc(&dn, sizeof(Norm));
+  if (e == cudaSuccess) e = cudaMalloc(&hist, sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&it, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dn, &hn, sizeof(Norm), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, sizeof(float), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(it, 0, sizeof(int), s);
+  if (e == cudaSuccess) e = loss_grad(out, tgt, batch, w, h, dn, static_cast<__nv_bfloat16*>(dz), hist, it, s);
+  float hl = 0.f;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hl, hist, sizeof(float), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dn);
+  cudaFree(hist);
+  cudaFree(it);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return PMHD_ERR_CUDA;
+  }
+  *loss = hl;
+  return PMHD_OK;
 }
 
 }  // extern "C"

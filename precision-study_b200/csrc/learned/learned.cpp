@@ -162,10 +162,13 @@ int pmhd_learned_destroy(pmhd_learned* L) {
   if (!L) return PMHD_OK;
   cudaSetDevice(L->cfg.device);
   if (L->stream) cudaStreamSynchronize(L->stream);
-  void* ptrs[] = {L->w.theta, L->w.wf[0], L->w.wf[1], L->w.wf[2], L->w.wb[0], L->w.wb[1], L->w.wb[2], L->grad,
-                  L->m,       L->v,       L->dnorm,   L->px,      L->py,      L->pz,      L->err};
+  void* ptrs[] = {L->w.theta, L->grad, L->m, L->v, L->dnorm, L->px, L->py, L->pz, L->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (int l = 0; l < kLayers; l++) {
+    if (L->w.wf[l]) cudaFree(L->w.wf[l]);
+    if (L->w.wb[l]) cudaFree(L->w.wb[l]);
+  }
   if (L->stream) cudaStreamDestroy(L->stream);
   delete L;
   return PMHD_OK;
@@ -203,7 +206,7 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
   ok = ok && dalloc(&L->w.theta, np) == cudaSuccess && dalloc(&L->grad, np) == cudaSuccess &&
        dalloc(&L->m, np) == cudaSuccess && dalloc(&L->v, np) == cudaSuccess && dalloc(&L->dnorm, 1) == cudaSuccess &&
        dalloc(&L->err, 1) == cudaSuccess;
-  for (int l = 0; ok && l < 3; l++) {
+  for (int l = 0; ok && l < kLayers; l++) {
     const size_t n = (size_t)L->L.cout[l] * 9 * L->L.cin[l];
     ok = dalloc(&L->w.wf[l], n) == cudaSuccess && dalloc(&L->w.wb[l], n) == cudaSuccess;
   }
@@ -219,9 +222,10 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
   // the last layer starts near zero so the untrained correction is ~0.
   std::vector<float> th(np, 0.f);
   unsigned long long st = cfg->seed;
-  const int used_in[3] = {2 * kNVar, kWidth, kWidth}, used_out[3] = {kWidth, kWidth, kNVar};
-  for (int l = 0; l < 3; l++) {
-    const double sd = (l < 2 ? std::sqrt(2.0 / (9.0 * used_in[l])) : 0.01 * std::sqrt(1.0 / (9.0 * used_in[l])));
+  const int used_in[kLayers] = {2 * kNVar, kWidth, kWidth, kWidth}, used_out[kLayers] = {kWidth, kWidth, kWidth, 8};
+  for (int l = 0; l < kLayers; l++) {
+    const double sd = (l < kLayers - 1 ? std::sqrt(2.0 / (9.0 * used_in[l]))
+                                       : 0.01 * std::sqrt(1.0 / (9.0 * used_in[l])));
     for (int co = 0; co < L->L.cout[l]; co++)
       for (int t = 0; t < 9; t++)
         for (int ci = 0; ci < L->L.cin[l]; ci++) {
@@ -359,37 +363,46 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
   // Normalisation from all pairs, fixed at the first training.
   if (!L->have_norm) {
     double* dsum = nullptr;
-    L_CU(dalloc(&dsum, 6 * kNVar));
-    L_CU(cudaMemsetAsync(dsum, 0, 6 * kNVar * sizeof(double), s));
-    L_CU(moments(aos_view(L->px, nx, ny), aos_view(L->py, nx, ny), aos_view(L->pz, nx, ny), np, nx, ny, dsum, s));
-    double h[6 * kNVar];
+    L_CU(dalloc(&dsum, kMomentSums));
+    L_CU(cudaMemsetAsync(dsum, 0, kMomentSums * sizeof(double), s));
+    L_CU(moments(aos_view(L->px, nx, ny), aos_view(L->py, nx, ny), aos_view(L->pz, nx, ny), np, nx, ny, L->cfg.gamma,
+                 dsum, s));
+    double h[kMomentSums];
     L_CU(cudaMemcpyAsync(h, dsum, sizeof(h), cudaMemcpyDeviceToHost, s));
     L_CU(cudaStreamSynchronize(s));
     cudaFree(dsum);
     const double n = (double)np * pix;
-    for (int g = 0; g < 3; g++)
+    for (int g = 0; g < 2; g++)
       for (int k = 0; k < kNVar; k++) {
         const double mean = h[g * kNVar + k] / n;
-        const double var = std::fmax(h[3 * kNVar + g * kNVar + k] / n - mean * mean, 0.0);
+        const double var = std::fmax(h[2 * kNVar + g * kNVar + k] / n - mean * mean, 0.0);
         const double sd = std::sqrt(var);
         const bool live = sd > 1e-12 * (1.0 + std::fabs(mean));
-        if (g < 2) {
-          L->hnorm.mu[g * kNVar + k] = (float)mean;
-          L->hnorm.inv_sig[g * kNVar + k] = live ? (float)(1.0 / sd) : 0.f;
-        } else {  // corrections: scale only, no shift
-          const double rms = std::sqrt(h[3 * kNVar + g * kNVar + k] / n);
-          const bool lv = rms > 1e-14;
-          L->hnorm.sig_out[k] = lv ? (float)rms : 0.f;
-          L->hnorm.inv_out[k] = lv ? (float)(1.0 / rms) : 0.f;
-        }
+        L->hnorm.mu[g * kNVar + k] = (float)mean;
+        L->hnorm.inv_sig[g * kNVar + k] = live ? (float)(1.0 / sd) : 0.f;
       }
+    // Corrections: scale only (root mean square), no shift.  Both field
+    // components share one scale so the curl of the potential is one map.
+    double rms[kNOutQ];
+    for (int k = 0; k < kNOutQ; k++) rms[k] = std::sqrt(std::fmax(h[4 * kNVar + kNOutQ + k] / n, 0.0));
+    const double rb = std::sqrt(0.5 * (rms[TGT_DBX] * rms[TGT_DBX] + rms[TGT_DBY] * rms[TGT_DBY]));
+    rms[TGT_DBX] = rms[TGT_DBY] = rb;
+    const double dx = (L->cfg.x_max - L->cfg.x_min) / nx, dy = (L->cfg.y_max - L->cfg.y_min) / ny;
+    rms[OUT_A] = rb * std::fmin(dx, dy);
+    for (int k = 0; k < kNOutQ; k++) {
+      const bool lv = rms[k] > 1e-14;
+      L->hnorm.sig_out[k] = lv ? (float)rms[k] : 0.f;
+      L->hnorm.inv_out[k] = lv ? (float)(1.0 / rms[k]) : 0.f;
+    }
+    L->hnorm.cx = rb > 1e-14 ? (float)(rms[OUT_A] / (2.0 * dx * rb)) : 0.f;
+    L->hnorm.cy = rb > 1e-14 ? (float)(rms[OUT_A] / (2.0 * dy * rb)) : 0.f;
     L_CU(cudaMemcpyAsync(L->dnorm, &L->hnorm, sizeof(Norm), cudaMemcpyHostToDevice, s));
     L_CU(cudaStreamSynchronize(s));
     L->have_norm = true;
   }
   // Network inputs and targets of every pair.
   __nv_bfloat16 *feat_all = nullptr, *xb = nullptr, *z1 = nullptr, *a1 = nullptr, *z2 = nullptr, *a2 = nullptr,
-                *dz3 = nullptr, *dz2 = nullptr, *dz1 = nullptr;
+                *z3 = nullptr, *a3 = nullptr, *dz4 = nullptr, *dz3 = nullptr, *dz2 = nullptr, *dz1 = nullptr;
   float *tgt_all = nullptr, *tb = nullptr, *out = nullptr, *hist = nullptr;
   int *sched = nullptr, *it = nullptr;
   std::vector<void*> owned;
@@ -402,7 +415,9 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
   ok = ok && grab(dalloc(&xb, (size_t)P * kFeat), xb) && grab(dalloc(&tb, (size_t)P * kOut), tb);
   ok = ok && grab(dalloc(&z1, (size_t)P * kWidth), z1) && grab(dalloc(&a1, (size_t)P * kWidth), a1);
   ok = ok && grab(dalloc(&z2, (size_t)P * kWidth), z2) && grab(dalloc(&a2, (size_t)P * kWidth), a2);
-  ok = ok && grab(dalloc(&out, (size_t)P * kOut), out) && grab(dalloc(&dz3, (size_t)P * kOut), dz3);
+  ok = ok && grab(dalloc(&z3, (size_t)P * kWidth), z3) && grab(dalloc(&a3, (size_t)P * kWidth), a3);
+  ok = ok && grab(dalloc(&out, (size_t)P * kOut), out) && grab(dalloc(&dz4, (size_t)P * kOut), dz4);
+  ok = ok && grab(dalloc(&dz3, (size_t)P * kWidth), dz3);
   ok = ok && grab(dalloc(&dz2, (size_t)P * kWidth), dz2) && grab(dalloc(&dz1, (size_t)P * kWidth), dz1);
   ok = ok && grab(dalloc(&hist, (size_t)iters), hist) && grab(dalloc(&sched, (size_t)iters * batch), sched);
   ok = ok && grab(dalloc(&it, 1), it);
@@ -424,7 +439,8 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
   if (e == cudaSuccess) e = cudaMemsetAsync(L->err, 0, sizeof(int), s);
   if (e == cudaSuccess)
     e = features(aos_view(L->py, nx, ny), aos_view(L->px, nx, ny), np, nx, ny, L->dnorm, feat_all, s);
-  if (e == cudaSuccess) e = targets(aos_view(L->py, nx, ny), aos_view(L->pz, nx, ny), np, nx, ny, L->dnorm, tgt_all, s);
+  if (e == cudaSuccess)
+    e = targets(aos_view(L->py, nx, ny), aos_view(L->pz, nx, ny), np, nx, ny, L->dnorm, L->cfg.gamma, tgt_all, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   // One training iteration, captured once and replayed.
   const NetLayout& N = L->L;
@@ -437,12 +453,17 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
     if (r == cudaSuccess)
       r = conv3x3(CONV_GELU, a1, batch, ny, nx, kWidth, L->w.wf[1], th + N.b_off[1], kWidth, nullptr, z2, a2, L->err, s);
     if (r == cudaSuccess)
-      r = conv3x3(CONV_LINEAR, a2, batch, ny, nx, kWidth, L->w.wf[2], th + N.b_off[2], kOut, nullptr, out, nullptr,
-                  L->err, s);
-    if (r == cudaSuccess) r = loss_grad(out, tb, P, dz3, hist, it, s);
-    if (r == cudaSuccess) r = conv3x3_wgrad(a2, dz3, batch, ny, nx, kWidth, kOut, g + N.w_off[2], g + N.b_off[2], L->err, s);
+      r = conv3x3(CONV_GELU, a2, batch, ny, nx, kWidth, L->w.wf[2], th + N.b_off[2], kWidth, nullptr, z3, a3, L->err, s);
     if (r == cudaSuccess)
-      r = conv3x3(CONV_DGELU, dz3, batch, ny, nx, kOut, L->w.wb[2], nullptr, kWidth, z2, dz2, nullptr, L->err, s);
+      r = conv3x3(CONV_LINEAR, a3, batch, ny, nx, kWidth, L->w.wf[3], th + N.b_off[3], kOut, nullptr, out, nullptr,
+                  L->err, s);
+    if (r == cudaSuccess) r = loss_grad(out, tb, batch, nx, ny, L->dnorm, dz4, hist, it, s);
+    if (r == cudaSuccess) r = conv3x3_wgrad(a3, dz4, batch, ny, nx, kWidth, kOut, g + N.w_off[3], g + N.b_off[3], L->err, s);
+    if (r == cudaSuccess)
+      r = conv3x3(CONV_DGELU, dz4, batch, ny, nx, kOut, L->w.wb[3], nullptr, kWidth, z3, dz3, nullptr, L->err, s);
+    if (r == cudaSuccess) r = conv3x3_wgrad(a2, dz3, batch, ny, nx, kWidth, kWidth, g + N.w_off[2], g + N.b_off[2], L->err, s);
+    if (r == cudaSuccess)
+      r = conv3x3(CONV_DGELU, dz3, batch, ny, nx, kWidth, L->w.wb[2], nullptr, kWidth, z2, dz2, nullptr, L->err, s);
     if (r == cudaSuccess) r = conv3x3_wgrad(a1, dz2, batch, ny, nx, kWidth, kWidth, g + N.w_off[1], g + N.b_off[1], L->err, s);
     if (r == cudaSuccess)
       r = conv3x3(CONV_DGELU, dz2, batch, ny, nx, kWidth, L->w.wb[1], nullptr, kWidth, z1, dz1, nullptr, L->err, s);
@@ -504,6 +525,7 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
   ok = ok && grab(dalloc(&cs.x, (size_t)pix * kFeat), cs.x) && grab(dalloc(&cs.z1, (size_t)pix * kWidth), cs.z1);
   ok = ok && grab(dalloc(&cs.a1, (size_t)pix * kWidth), cs.a1) && grab(dalloc(&cs.z2, (size_t)pix * kWidth), cs.z2);
   ok = ok && grab(dalloc(&cs.a2, (size_t)pix * kWidth), cs.a2) && grab(dalloc(&cs.out, (size_t)pix * kOut), cs.out);
+  ok = ok && grab(dalloc(&cs.z3, (size_t)pix * kWidth), cs.z3) && grab(dalloc(&cs.a3, (size_t)pix * kWidth), cs.a3);
   ok = ok && grab(dalloc(&cs.flags, 4), cs.flags) && grab(dalloc(&cs.sums, 4), cs.sums);
   ok = ok && grab(dalloc(&cs.counters, 4), cs.counters) && grab(dalloc(&cs.accept, 4), cs.accept);
   auto release = [&]() {
@@ -550,7 +572,10 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
         r = conv3x3(CONV_GELU, cs.a1, 1, ny, nx, kWidth, W.wf[1], W.theta + N.b_off[1], kWidth, nullptr, cs.z2, cs.a2,
                     err, s);
       if (r == cudaSuccess)
-        r = conv3x3(CONV_LINEAR, cs.a2, 1, ny, nx, kWidth, W.wf[2], W.theta + N.b_off[2], kOut, nullptr, cs.out,
+        r = conv3x3(CONV_GELU, cs.a2, 1, ny, nx, kWidth, W.wf[2], W.theta + N.b_off[2], kWidth, nullptr, cs.z3, cs.a3,
+                    err, s);
+      if (r == cudaSuccess)
+        r = conv3x3(CONV_LINEAR, cs.a3, 1, ny, nx, kWidth, W.wf[3], W.theta + N.b_off[3], kOut, nullptr, cs.out,
                     nullptr, err, s);
       if (r == cudaSuccess)
         r = correct_step(cs, vc.u, vc.pitch, vc.plane, nx, ny, vc.dx, vc.dy, vc.gamma, div_tol, vc.ctrl, vc.ctrl, p, s);
@@ -615,7 +640,8 @@ int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, in
   return e == cudaSuccess ? PMHD_OK : PMHD_ERR_CUDA;
 }
 
-// File: "PMHDNET1", int32 n_params, Norm, n_params floats.
+// File: "PMHDNET2", int32 n_params, Norm, n_params floats (four layers,
+// physical-quantity outputs).
 int pmhd_learned_save(const pmhd_learned* L, const char* path) {
   if (!L || !path || !L->have_norm) return PMHD_ERR_ARG;
   std::vector<float> th(L->L.n_params);
@@ -626,7 +652,7 @@ int pmhd_learned_save(const pmhd_learned* L, const char* path) {
   FILE* f = std::fopen(path, "wb");
   if (!f) return PMHD_ERR_IO;
   const int n = L->L.n_params;
-  bool ok = std::fwrite("PMHDNET1", 1, 8, f) == 8 && std::fwrite(&n, sizeof(int), 1, f) == 1 &&
+  bool ok = std::fwrite("PMHDNET2", 1, 8, f) == 8 && std::fwrite(&n, sizeof(int), 1, f) == 1 &&
             std::fwrite(&L->hnorm, sizeof(Norm), 1, f) == 1 &&
             std::fwrite(th.data(), sizeof(float), th.size(), f) == th.size();
   ok = (std::fclose(f) == 0) && ok;
@@ -641,7 +667,7 @@ int pmhd_learned_load(pmhd_learned* L, const char* path) {
   int n = 0;
   Norm nm;
   std::vector<float> th(L->L.n_params);
-  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PMHDNET1", 8) == 0 &&
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PMHDNET2", 8) == 0 &&
             std::fread(&n, sizeof(int), 1, f) == 1 && n == L->L.n_params &&
             std::fread(&nm, sizeof(Norm), 1, f) == 1 && std::fread(th.data(), sizeof(float), th.size(), f) == th.size();
   std::fclose(f);

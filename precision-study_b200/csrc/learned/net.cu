@@ -16,9 +16,9 @@ namespace learned {
 
 NetLayout net_layout() {
   NetLayout L{};
-  const int cin[3] = {kFeat, kWidth, kWidth}, cout[3] = {kWidth, kWidth, kOut};
+  const int cin[kLayers] = {kFeat, kWidth, kWidth, kWidth}, cout[kLayers] = {kWidth, kWidth, kWidth, kOut};
   int off = 0;
-  for (int l = 0; l < 3; l++) {
+  for (int l = 0; l < kLayers; l++) {
     L.cin[l] = cin[l];
     L.cout[l] = cout[l];
     L.w_off[l] = off;
@@ -64,33 +64,68 @@ __global__ void features_kernel(StateView after, StateView before, int batch, in
   }
 }
 
+// Primitives of one cell of a state view (rho, vx, vy, vz, p, Bx, By, Bz, psi).
+__device__ __forceinline__ void prim_at(const StateView& s, long long b, int i, int j, double gamma, double* w) {
+  double U[kNVar];
+#pragma unroll
+  for (int k = 0; k < kNVar; k++) U[k] = sv(s, b, k, i, j);
+  const double inv = 1.0 / U[0];
+  w[0] = U[0];
+  w[1] = U[1] * inv;
+  w[2] = U[2] * inv;
+  w[3] = U[3] * inv;
+  w[4] = (gamma - 1.0) * (U[4] - 0.5 * U[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]) -
+                          0.5 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7]));
+  w[5] = U[5];
+  w[6] = U[6];
+  w[7] = U[7];
+  w[8] = U[8];
+}
+
+// Target quantities (Out order) of the change from state a to state f; the
+// logarithms need positive densities and pressures (usable states), else 0.
+__device__ __forceinline__ void target_q(const double* a, const double* f, double* q) {
+  q[OUT_LRHO] = (a[0] > 0.0 && f[0] > 0.0) ? log(f[0] / a[0]) : 0.0;
+  q[OUT_V] = f[1] - a[1];
+  q[OUT_V + 1] = f[2] - a[2];
+  q[OUT_V + 2] = f[3] - a[3];
+  q[OUT_LP] = (a[4] > 0.0 && f[4] > 0.0) ? log(f[4] / a[4]) : 0.0;
+  q[OUT_A] = 0.0;
+  q[OUT_BZ] = f[7] - a[7];
+  q[OUT_PSI] = f[8] - a[8];
+  q[TGT_DBX] = f[5] - a[5];
+  q[TGT_DBY] = f[6] - a[6];
+}
+
 __global__ void targets_kernel(StateView after, StateView fine, int batch, int nx, int ny,
-                               const Norm* __restrict__ norm, float* __restrict__ tgt) {
+                               const Norm* __restrict__ norm, double gamma, float* __restrict__ tgt) {
   const long long P = (long long)batch * nx * ny;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx);
     const long long r = q / nx;
     const int j = (int)(r % ny);
     const long long b = r / ny;
+    double a[kNVar], f[kNVar], t[kNOutQ];
+    prim_at(after, b, i, j, gamma, a);
+    prim_at(fine, b, i, j, gamma, f);
+    target_q(a, f, t);
     float* o = tgt + q * kOut;
 #pragma unroll
-    for (int k = 0; k < kNVar; k++) {
-      const double d = sv(fine, b, k, i, j) - sv(after, b, k, i, j);
-      o[k] = (float)d * norm->inv_out[k];
-    }
+    for (int k = 0; k < kNOutQ; k++) o[k] = (float)t[k] * norm->inv_out[k];
 #pragma unroll
-    for (int k = kNVar; k < kOut; k++) o[k] = 0.f;
+    for (int k = kNOutQ; k < kOut; k++) o[k] = 0.f;
   }
 }
 
 __global__ void moments_kernel(StateView before, StateView after, StateView fine, int batch, int nx, int ny,
-                               double* __restrict__ sums) {
-  __shared__ double part[6 * kNVar];
-  for (int k = threadIdx.x; k < 6 * kNVar; k += blockDim.x) part[k] = 0.0;
+                               double gamma, double* __restrict__ sums) {
+  constexpr int NS = kMomentSums;
+  __shared__ double part[NS];
+  for (int k = threadIdx.x; k < NS; k += blockDim.x) part[k] = 0.0;
   __syncthreads();
-  double acc[6 * kNVar];
+  double acc[NS];
 #pragma unroll
-  for (int k = 0; k < 6 * kNVar; k++) acc[k] = 0.0;
+  for (int k = 0; k < NS; k++) acc[k] = 0.0;
   const long long P = (long long)batch * nx * ny;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx);
@@ -99,35 +134,65 @@ __global__ void moments_kernel(StateView before, StateView after, StateView fine
     const long long b = r / ny;
 #pragma unroll
     for (int k = 0; k < kNVar; k++) {
-      const double a = sv(after, b, k, i, j);
-      const double v[3] = {a, a - sv(before, b, k, i, j), sv(fine, b, k, i, j) - a};
+      const double a = sv(after, b, k, i, j), d = a - sv(before, b, k, i, j);
+      acc[k] += a;
+      acc[kNVar + k] += d;
+      acc[2 * kNVar + k] += a * a;
+      acc[3 * kNVar + k] += d * d;
+    }
+    double pa[kNVar], pf[kNVar], t[kNOutQ];
+    prim_at(after, b, i, j, gamma, pa);
+    prim_at(fine, b, i, j, gamma, pf);
+    target_q(pa, pf, t);
 #pragma unroll
-      for (int g = 0; g < 3; g++) {
-        acc[g * kNVar + k] += v[g];
-        acc[3 * kNVar + g * kNVar + k] += v[g] * v[g];
-      }
+    for (int k = 0; k < kNOutQ; k++) {
+      acc[4 * kNVar + k] += t[k];
+      acc[4 * kNVar + kNOutQ + k] += t[k] * t[k];
     }
   }
 #pragma unroll
-  for (int k = 0; k < 6 * kNVar; k++) atomicAdd(&part[k], acc[k]);
+  for (int k = 0; k < NS; k++) atomicAdd(&part[k], acc[k]);
   __syncthreads();
-  for (int k = threadIdx.x; k < 6 * kNVar; k += blockDim.x) atomicAdd(&sums[k], part[k]);
+  for (int k = threadIdx.x; k < NS; k += blockDim.x) atomicAdd(&sums[k], part[k]);
 }
 
-__global__ void loss_grad_kernel(const float* __restrict__ out, const float* __restrict__ tgt, long long P,
-                                 __nv_bfloat16* __restrict__ dz, float* __restrict__ loss_hist,
-                                 const int* __restrict__ it) {
-  const float scale = 2.0f / (float)(P * kNVar);
+// Loss over the nine trained quantities: the seven direct channels and the
+// two field components, the latter through the curl of OUT_A (periodic on
+// each image).  With rx(q) = cy (A(q+j) - A(q-j)) - t_bx(q) and
+// ry(q) = -cx (A(q+i) - A(q-i)) - t_by(q), the gradient with respect to A at
+// q collects the terms of the four neighbours whose curls contain it.
+__global__ void loss_grad_kernel(const float* __restrict__ out, const float* __restrict__ tgt, int batch, int nx,
+                                 int ny, const Norm* __restrict__ norm, __nv_bfloat16* __restrict__ dz,
+                                 float* __restrict__ loss_hist, const int* __restrict__ it) {
+  const long long P = (long long)batch * nx * ny;
+  const float scale = 2.0f / (float)(P * 9);
+  const float cx = norm->cx, cy = norm->cy;
   float part = 0.f;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx);
+    const long long r = q / nx;
+    const int j = (int)(r % ny);
+    const long long img = r / ny;
+    auto at = [&](int ii, int jj) -> long long {
+      ii = (ii % nx + nx) % nx;
+      jj = (jj % ny + ny) % ny;
+      return (img * ny + jj) * nx + ii;
+    };
+    auto A = [&](int ii, int jj) { return out[at(ii, jj) * kOut + OUT_A]; };
+    auto rx = [&](int ii, int jj) { return cy * (A(ii, jj + 1) - A(ii, jj - 1)) - tgt[at(ii, jj) * kOut + TGT_DBX]; };
+    auto ry = [&](int ii, int jj) { return -cx * (A(ii + 1, jj) - A(ii - 1, jj)) - tgt[at(ii, jj) * kOut + TGT_DBY]; };
     __align__(16) __nv_bfloat16 g[kOut];
 #pragma unroll
     for (int k = 0; k < kOut; k++) {
       float d = 0.f;
-      if (k < kNVar) d = out[q * kOut + k] - tgt[q * kOut + k];
+      if (k < 8 && k != OUT_A) d = out[q * kOut + k] - tgt[q * kOut + k];
       part += d * d;
       g[k] = __float2bfloat16_rn(scale * d);
     }
+    const float rxq = rx(i, j), ryq = ry(i, j);
+    part += rxq * rxq + ryq * ryq;
+    const float ga = cy * (rx(i, j - 1) - rx(i, j + 1)) + cx * (ry(i + 1, j) - ry(i - 1, j));
+    g[OUT_A] = __float2bfloat16_rn(scale * ga);
     uint4* dst = reinterpret_cast<uint4*>(dz + q * kOut);
     dst[0] = reinterpret_cast<const uint4*>(g)[0];
     dst[1] = reinterpret_cast<const uint4*>(g)[1];
@@ -139,7 +204,7 @@ __global__ void loss_grad_kernel(const float* __restrict__ out, const float* __r
   if (threadIdx.x == 0) {
     float s = 0.f;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
-    atomicAdd(loss_hist + *it, s / (float)(P * kNVar));
+    atomicAdd(loss_hist + *it, s / (float)(P * 9));
   }
 }
 
@@ -147,7 +212,7 @@ __global__ void loss_grad_kernel(const float* __restrict__ out, const float* __r
 // weight).
 __device__ __forceinline__ void write_bf16(const NetLayout& L, const NetWeights& w, int e, float th) {
 #pragma unroll
-  for (int l = 0; l < 3; l++) {
+  for (int l = 0; l < kLayers; l++) {
     const int n = L.cout[l] * 9 * L.cin[l];
     const int q = e - L.w_off[l];
     if (q >= 0 && q < n) {
@@ -245,28 +310,52 @@ __global__ void store_interior_kernel(const double* __restrict__ u, int pitch, l
   }
 }
 
-// Candidate = state after the step + sig_out * network output; flags a
-// cell whose density or pressure is not positive (or not finite).
+// Candidate = the state after the step corrected by the network output:
+// density and pressure scaled by exp(correction) (the exponent clamped to
+// [-2, 2]), velocities, B_z and psi shifted, B_x and B_y shifted by the
+// central-difference curl of the potential (periodic); flags a cell whose
+// density or pressure is not positive (or not finite).
 __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long long plane, int nx, int ny,
                                  const float* __restrict__ out, const Norm* __restrict__ norm, double gamma,
-                                 double* __restrict__ cand, int* __restrict__ flags, const Ctrl* __restrict__ c,
-                                 int p) {
+                                 double dx, double dy, double* __restrict__ cand, int* __restrict__ flags,
+                                 const Ctrl* __restrict__ c, int p) {
   if (!step_taken(c, p)) return;
   const long long n = (long long)nx * ny;
   int bad = 0;
+  const double sA = norm->sig_out[OUT_A];
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx), j = (int)(q / nx);
     double U[kNVar];
 #pragma unroll
-    for (int k = 0; k < kNVar; k++) {
-      U[k] = u[k * plane + (long long)(j + 2) * pitch + (i + 2)] + (double)norm->sig_out[k] * (double)out[q * kOut + k];
-      cand[q * kNVar + k] = U[k];
-    }
-    const double rho = U[0];
-    const double ke = 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rho;
-    const double me = 0.5 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7]);
-    const double pr = (gamma - 1.0) * (U[4] - ke - me);
-    if (!(rho > 0.0) || !(pr > 0.0) || !isfinite(pr)) bad = 1;
+    for (int k = 0; k < kNVar; k++) U[k] = u[k * plane + (long long)(j + 2) * pitch + (i + 2)];
+    const float* o = out + q * kOut;
+    auto sig = [&](int k) { return (double)norm->sig_out[k] * (double)o[k]; };
+    auto clamp2 = [](double x) { return x < -2.0 ? -2.0 : (x > 2.0 ? 2.0 : x); };
+    const double rho = U[0], inv = 1.0 / rho;
+    const double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
+    const double pr = (gamma - 1.0) * (U[4] - 0.5 * rho * (vx * vx + vy * vy + vz * vz) -
+                                       0.5 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7]));
+    const double rho1 = rho * exp(clamp2(sig(OUT_LRHO)));
+    const double vx1 = vx + sig(OUT_V), vy1 = vy + sig(OUT_V + 1), vz1 = vz + sig(OUT_V + 2);
+    const double p1 = pr * exp(clamp2(sig(OUT_LP)));
+    const int ip = (i + 1) % nx, im = (i + nx - 1) % nx, jp = (j + 1) % ny, jm = (j + ny - 1) % ny;
+    const double a_n = sA * out[((long long)jp * nx + i) * kOut + OUT_A], a_s = sA * out[((long long)jm * nx + i) * kOut + OUT_A];
+    const double a_e = sA * out[((long long)j * nx + ip) * kOut + OUT_A], a_w = sA * out[((long long)j * nx + im) * kOut + OUT_A];
+    const double bx1 = U[5] + (a_n - a_s) / (2.0 * dy), by1 = U[6] - (a_e - a_w) / (2.0 * dx);
+    const double bz1 = U[7] + sig(OUT_BZ), psi1 = U[8] + sig(OUT_PSI);
+    double* C = cand + q * kNVar;
+    C[0] = rho1;
+    C[1] = rho1 * vx1;
+    C[2] = rho1 * vy1;
+    C[3] = rho1 * vz1;
+    C[4] = p1 / (gamma - 1.0) + 0.5 * rho1 * (vx1 * vx1 + vy1 * vy1 + vz1 * vz1) +
+           0.5 * (bx1 * bx1 + by1 * by1 + bz1 * bz1);
+    C[5] = bx1;
+    C[6] = by1;
+    C[7] = bz1;
+    C[8] = psi1;
+    if (!(rho1 > 0.0) || !(p1 > 0.0) || !isfinite(C[4]) || !isfinite(C[1] + C[2] + C[3] + C[5] + C[6] + C[8]))
+      bad = 1;
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1);
 }
@@ -347,20 +436,23 @@ cudaError_t features(const StateView& after, const StateView& before, int batch,
 }
 
 cudaError_t targets(const StateView& after, const StateView& fine, int batch, int nx, int ny, const Norm* norm,
-                    float* tgt, cudaStream_t s) {
-  targets_kernel<<<grid_for((long long)batch * nx * ny, 256), 256, 0, s>>>(after, fine, batch, nx, ny, norm, tgt);
+                    double gamma, float* tgt, cudaStream_t s) {
+  targets_kernel<<<grid_for((long long)batch * nx * ny, 256), 256, 0, s>>>(after, fine, batch, nx, ny, norm, gamma,
+                                                                            tgt);
   return cudaGetLastError();
 }
 
 cudaError_t moments(const StateView& before, const StateView& after, const StateView& fine, int batch, int nx,
-                    int ny, double* sums, cudaStream_t s) {
-  moments_kernel<<<grid_for((long long)batch * nx * ny, 128), 128, 0, s>>>(before, after, fine, batch, nx, ny, sums);
+                    int ny, double gamma, double* sums, cudaStream_t s) {
+  moments_kernel<<<grid_for((long long)batch * nx * ny, 128), 128, 0, s>>>(before, after, fine, batch, nx, ny, gamma,
+                                                                            sums);
   return cudaGetLastError();
 }
 
-cudaError_t loss_grad(const float* out, const float* tgt, long long P, __nv_bfloat16* dz, float* loss_hist,
-                      const int* it, cudaStream_t s) {
-  loss_grad_kernel<<<grid_for(P, 256), 256, 0, s>>>(out, tgt, P, dz, loss_hist, it);
+cudaError_t loss_grad(const float* out, const float* tgt, int batch, int nx, int ny, const Norm* norm,
+                      __nv_bfloat16* dz, float* loss_hist, const int* it, cudaStream_t s) {
+  loss_grad_kernel<<<grid_for((long long)batch * nx * ny, 256), 256, 0, s>>>(out, tgt, batch, nx, ny, norm, dz,
+                                                                              loss_hist, it);
   return cudaGetLastError();
 }
 
@@ -415,8 +507,8 @@ cudaError_t correct_step(const CorrState& cs, void* u, int pitch, long long plan
                          cudaStream_t s) {
   double* ud = static_cast<double*>(u);
   const long long n = (long long)nx * ny;
-  candidate_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.out, cs.norm, gamma, cs.cand,
-                                                    cs.flags, ctrl, p);
+  candidate_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.out, cs.norm, gamma, dx, dy,
+                                                    cs.cand, cs.flags, ctrl, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   divnorm_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.cand, dx, dy, cs.sums, ctrl, p);

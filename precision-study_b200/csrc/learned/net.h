@@ -15,7 +15,21 @@ namespace learned {
 constexpr int kNVar = 9;
 constexpr int kFeat = 32;   // input channels (18 used: state and step increment)
 constexpr int kWidth = 32;  // hidden channels
-constexpr int kOut = 16;    // output channels (9 used: the correction)
+constexpr int kOut = 16;    // output channels (8 used: the correction, see Out)
+constexpr int kLayers = 4;  // 3x3 layers: 3 x (32 -> 32, GELU), 32 -> 16 linear
+
+// Output channels: the correction in quantities that keep it physical.
+//   OUT_LRHO / OUT_LP  log(rho_new / rho), log(p_new / p): positive by
+//                      construction;
+//   OUT_V..OUT_V+2     velocity increments;
+//   OUT_A              a vector potential A_z: the field changes by its
+//                      central-difference curl (dBx = dA/dy, dBy = -dA/dx), which
+//                      leaves the central-difference div B unchanged;
+//   OUT_BZ, OUT_PSI    increments of B_z and psi.
+// Target channels 8 and 9 hold the field change (dBx, dBy) the curl of OUT_A
+// is trained against.
+enum Out : int { OUT_LRHO = 0, OUT_V = 1, OUT_LP = 4, OUT_A = 5, OUT_BZ = 6, OUT_PSI = 7, TGT_DBX = 8, TGT_DBY = 9 };
+constexpr int kNOutQ = 10;  // target quantities (channels 0..9; 5 unused)
 
 // fp64 state of `batch` grids: variable k of interior cell (i, j) of grid b at
 // u[offset + b*bstride + k*vstride + j*jstride + i*istride].
@@ -34,13 +48,18 @@ inline StateView aos_view(const void* u, int nx, int ny) {
 // Normalisation of the network's inputs and outputs.
 struct Norm {
   float mu[2 * kNVar], inv_sig[2 * kNVar];  // features: state, step increment
-  float sig_out[kNVar], inv_out[kNVar];     // correction scale per variable (0 / 0: not corrected)
+  // Scale of each target quantity (0 / 0: not corrected).  For OUT_A the scale
+  // is that of the potential, sig_out[TGT_DBX] * min(dx, dy).
+  float sig_out[kNOutQ], inv_out[kNOutQ];
+  // curl of the normalised potential in normalised field units:
+  // dBx_n = cy * (A_n[j+1] - A_n[j-1]), dBy_n = -cx * (A_n[i+1] - A_n[i-1]).
+  float cx, cy;
 };
 
-// Three 3x3 layers: 32 -> 32 (GELU) -> 32 (GELU) -> 16 (linear).
+// Four 3x3 layers: 32 -> 32 -> 32 -> 32 (GELU) -> 16 (linear).
 struct NetLayout {
-  int w_off[3], b_off[3];  // offsets into the fp32 parameter vector
-  int cin[3], cout[3];
+  int w_off[kLayers], b_off[kLayers];  // offsets into the fp32 parameter vector
+  int cin[kLayers], cout[kLayers];
   int n_params;
 };
 NetLayout net_layout();
@@ -48,8 +67,8 @@ NetLayout net_layout();
 // Device pointers of one set of network weights.
 struct NetWeights {
   float* theta;                  // fp32 parameters (weights then bias per layer)
-  __nv_bfloat16* wf[3];          // bf16 [cout][9][cin] (forward)
-  __nv_bfloat16* wb[3];          // bf16 [cin][9][cout] (backward to the input)
+  __nv_bfloat16* wf[kLayers];    // bf16 [cout][9][cin] (forward)
+  __nv_bfloat16* wb[kLayers];    // bf16 [cin][9][cout] (backward to the input)
 };
 
 // Per-step work of a corrected run.
@@ -57,7 +76,7 @@ struct CorrState {
   double* before;      // SoA copy of the state before the step (solver layout)
   double* cand;        // AoS interior candidate state
   __nv_bfloat16* x;    // features [ny][nx][32]
-  __nv_bfloat16* z1, *a1, *z2, *a2;
+  __nv_bfloat16* z1, *a1, *z2, *a2, *z3, *a3;
   float* out;          // network output [ny][nx][16]
   // flags[0]: candidate not positive; sums[0..1]: ||divB||_1 after the step
   // and of the candidate; counters[0..2]: accepted, rejected (positivity),
@@ -71,14 +90,20 @@ struct CorrState {
 
 cudaError_t features(const StateView& after, const StateView& before, int batch, int nx, int ny, const Norm* norm,
                      __nv_bfloat16* x, cudaStream_t s);
+// Normalised target quantities (Out) of the step from `after` to `fine`.
 cudaError_t targets(const StateView& after, const StateView& fine, int batch, int nx, int ny, const Norm* norm,
-                    float* tgt, cudaStream_t s);
-// sums[0..26] += per-variable sums of (after, after - before, fine - after),
-// sums[27..53] += their squares.
+                    double gamma, float* tgt, cudaStream_t s);
+// sums[0..17] += per-variable sums of (after, after - before), sums[18..35]
+// += their squares; sums[36..45] += sums of the target quantities (Out,
+// unnormalised) from `after` to `fine`, sums[46..55] += their squares.
+constexpr int kMomentSums = 56;
 cudaError_t moments(const StateView& before, const StateView& after, const StateView& fine, int batch, int nx,
-                    int ny, double* sums, cudaStream_t s);
-cudaError_t loss_grad(const float* out, const float* tgt, long long P, __nv_bfloat16* dz, float* loss_hist,
-                      const int* it, cudaStream_t s);
+                    int ny, double gamma, double* sums, cudaStream_t s);
+// Mean squared error over the target quantities (the field through the curl
+// of OUT_A, periodic on each nx x ny image of the batch) and its gradient
+// with respect to the output.
+cudaError_t loss_grad(const float* out, const float* tgt, int batch, int nx, int ny, const Norm* norm,
+                      __nv_bfloat16* dz, float* loss_hist, const int* it, cudaStream_t s);
 cudaError_t adam(const NetLayout& L, NetWeights w, float* grad, float* m, float* v, const int* it, int iters,
                  float lr, cudaStream_t s);
 cudaError_t weights_to_bf16(const NetLayout& L, NetWeights w, cudaStream_t s);

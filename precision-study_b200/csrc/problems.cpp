@@ -75,7 +75,8 @@ bool init_problem_host(const ProblemGrid& g, int problem, const double* params, 
           P[8] = (T)0.0;
           break;
         case PMHD_PROBLEM_KH_REF: {  // mhd2d_glm_gpu.cu:421-441
-          const T a = (T)0.025, sigma = (T)0.05, delta = (T)0.01;
+          // params[0]: the shear-layer width (the reference's 0.025 when absent).
+          const T a = (params && nparams > 0) ? (T)params[0] : (T)0.025, sigma = (T)0.05, delta = (T)0.01;
           const T S = (T)0.5 * (t_tanh((y - (T)0.25) / a) - t_tanh((y - (T)0.75) / a));
           const T g1 = (y - (T)0.25) / sigma;
           const T g2 = (y - (T)0.75) / sigma;

@@ -41,7 +41,7 @@ EXPORTS = (
     "pmhd_strerror", "pmhd_get_config", "pmhd_problem_state", "pmhd_advance_noalloc",
     "pmhd_ensemble_describe_default", "pmhd_ensemble_create", "pmhd_ensemble_advance",
     "pmhd_ensemble_member_stats", "pmhd_ensemble_get_state", "pmhd_ensemble_destroy",
-    "pmhd_conv3x3", "pmhd_conv3x3_wgrad",
+    "pmhd_conv3x3", "pmhd_conv3x3_wgrad", "pmhd_learned_loss_grad",
     "pmhd_learned_config_default", "pmhd_learned_create", "pmhd_learned_destroy", "pmhd_learned_generate",
     "pmhd_learned_generate_rollout",
     "pmhd_learned_num_pairs", "pmhd_learned_train", "pmhd_learned_run", "pmhd_learned_fine_run",
@@ -172,6 +172,7 @@ def load():
         "pmhd_ensemble_destroy": ([vp], i),
         "pmhd_conv3x3": ([i, vp, i, i, i, i, vp, P(ctypes.c_float), i, vp, vp, vp, vp], i),
         "pmhd_conv3x3_wgrad": ([vp, vp, i, i, i, i, i, P(ctypes.c_float), P(ctypes.c_float), vp], i),
+        "pmhd_learned_loss_grad": ([vp, vp, i, i, i, ctypes.c_float, ctypes.c_float, vp, P(d), vp], i),
         "pmhd_learned_config_default": ([P(LearnedConfig)], i),
         "pmhd_learned_create": ([P(LearnedConfig), P(vp)], i),
         "pmhd_learned_destroy": ([vp], i),

@@ -1,5 +1,6 @@
 """GPU checks of the BF16 tensor-core convolutions (pmhd_conv3x3,
-pmhd_conv3x3_wgrad) against the float64 network oracle.
+pmhd_conv3x3_wgrad) and the training loss (pmhd_learned_loss_grad) against
+the float64 network oracle, and of the trained correction.
 
 Two kinds of case per kernel: small-integer data, for which every product
 and partial sum is exact in the kernels' fp32 accumulators, so the results
@@ -176,34 +177,62 @@ def test_unsupported_channel_counts_are_rejected(pmhd_lib):
     assert rc == pmhd_lib.ERR_UNSUPPORTED
 
 
-def test_network_gradient_chain_matches_oracle(pmhd_lib):
-    """The training iteration's chain (forward GELU, GELU, linear; loss
-    gradient; weight gradients; backward through both GELUs) composed from
-    the kernels matches the float64 oracle's analytic gradients."""
+def _loss_grad(pmhd, out, tgt, cx, cy):
     import torch
+    B, H, Wd, _ = out.shape
+    od, td = _dev_f32(out), _dev_f32(tgt)
+    dz = torch.zeros((B, H, Wd, 16), dtype=torch.bfloat16, device="cuda")
+    loss = ctypes.c_double()
+    rc = pmhd.load().pmhd_learned_loss_grad(od.data_ptr(), td.data_ptr(), B, H, Wd, cx, cy, dz.data_ptr(),
+                                            ctypes.byref(loss), None)
+    assert rc == pmhd.OK, pmhd.strerror(rc)
+    return loss.value, _host(dz)
+
+
+def test_loss_kernel_matches_oracle(pmhd_lib):
+    """The training loss and its gradient (direct channels and the field
+    through the curl of the potential channel, periodic) against the float64
+    oracle, on a batch with partial sizes; dz is bf16 (8 significant bits)."""
+    rng = np.random.default_rng(31)
+    out = rng.normal(0, 1, (3, 17, 23, 16)).astype(np.float32).astype(np.float64)
+    tgt = rng.normal(0, 1, (3, 17, 23, 16)).astype(np.float32).astype(np.float64)
+    cx, cy = 0.5, 0.625
+    loss, dz = _loss_grad(pmhd_lib, out, tgt, cx, cy)
+    rl, rg = C.curl_loss_and_grad(out, tgt, cx, cy)
+    assert abs(loss - rl) < 1e-5 * rl
+    np.testing.assert_allclose(dz, rg, rtol=2.0 ** -7, atol=1e-3 * np.abs(rg).max())
+    assert np.all(dz[..., 8:] == 0)
+
+
+def test_network_gradient_chain_matches_oracle(pmhd_lib):
+    """The training iteration's chain (four layers: GELU, GELU, GELU, linear;
+    the loss kernel's gradient; weight gradients; backward through the three
+    GELUs) composed from the kernels matches the float64 oracle's analytic
+    gradients."""
     rng = np.random.default_rng(21)
     shape = (2, 16, 24)
-    P = shape[0] * shape[1] * shape[2]
     x = _bf(np.concatenate([rng.normal(0, 1, shape + (18,)), np.zeros(shape + (14,))], axis=3))
-    W1 = _bf(rng.normal(0, 0.1, (32, 9, 32)))
-    W2 = _bf(rng.normal(0, 0.1, (32, 9, 32)))
-    W3 = _bf(rng.normal(0, 0.1, (16, 9, 32)))
-    b1, b2, b3 = (rng.normal(0, 0.05, n).astype(np.float32).astype(np.float64) for n in (32, 32, 16))
-    tgt = rng.normal(0, 1, shape + (16,))
-    tgt[..., 9:] = 0
+    W1, W2, W3 = (_bf(rng.normal(0, 0.1, (32, 9, 32))) for _ in range(3))
+    W4 = _bf(rng.normal(0, 0.1, (16, 9, 32)))
+    b1, b2, b3, b4 = (rng.normal(0, 0.05, n).astype(np.float32).astype(np.float64) for n in (32, 32, 32, 16))
+    tgt = rng.normal(0, 1, shape + (16,)).astype(np.float32).astype(np.float64)
+    tgt[..., 10:] = 0
+    tgt[..., 5] = 0
+    cx, cy = 0.5, 0.5
     z1, a1 = _conv(pmhd_lib, pmhd_lib.CONV_GELU, x, W1, b1, 32)
     z2, a2 = _conv(pmhd_lib, pmhd_lib.CONV_GELU, a1, W2, b2, 32)
-    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_LINEAR, a2, W3, b3, 16)
-    d = out - tgt
-    d[..., 9:] = 0
-    dz3 = _bf(2.0 * d / (P * 9))
+    z3, a3 = _conv(pmhd_lib, pmhd_lib.CONV_GELU, a2, W3, b3, 32)
+    out, _ = _conv(pmhd_lib, pmhd_lib.CONV_LINEAR, a3, W4, b4, 16)
+    _, dz4 = _loss_grad(pmhd_lib, out, tgt, cx, cy)
+    gW4, gb4 = _wgrad(pmhd_lib, a3, dz4)
+    dz3, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz4, np.ascontiguousarray(W4.transpose(2, 1, 0)), None, 32, zprev=z3)
     gW3, gb3 = _wgrad(pmhd_lib, a2, dz3)
     dz2, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz3, np.ascontiguousarray(W3.transpose(2, 1, 0)), None, 32, zprev=z2)
     gW2, gb2 = _wgrad(pmhd_lib, a1, dz2)
     dz1, _ = _conv(pmhd_lib, pmhd_lib.CONV_DGELU, dz2, np.ascontiguousarray(W2.transpose(2, 1, 0)), None, 32, zprev=z1)
     gW1, gb1 = _wgrad(pmhd_lib, x, dz1)
-    _, grads = C.net_loss_and_grads(x, [(W1, b1), (W2, b2), (W3, b3)], tgt, 9)
-    for (gw, gb), (rw, rb) in zip([(gW1, gb1), (gW2, gb2), (gW3, gb3)], grads):
+    _, grads = C.net_curl_loss_and_grads(x, [(W1, b1), (W2, b2), (W3, b3), (W4, b4)], tgt, cx, cy)
+    for (gw, gb), (rw, rb) in zip([(gW1, gb1), (gW2, gb2), (gW3, gb3), (gW4, gb4)], grads):
         # bf16 activations and gradients: a few per cent of the largest entry.
         np.testing.assert_allclose(gw, rw, rtol=0, atol=0.03 * np.abs(rw).max())
         np.testing.assert_allclose(gb, rb, rtol=0, atol=0.03 * np.abs(rb).max())

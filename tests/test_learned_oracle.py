@@ -81,3 +81,63 @@ def test_learned_config_defaults_and_argument_checks(pmhd_lib):
     assert L.pmhd_learned_train(None, 10, 4, 1e-3, None) == pmhd_lib.ERR_ARG
     assert L.pmhd_learned_destroy(None) == pmhd_lib.OK
     assert L.pmhd_learned_num_pairs(None) == 0
+
+
+def test_curl_loss_gradient_matches_finite_differences():
+    """The correction loss (direct channels plus the field through the curl
+    of the potential channel) against central finite differences in every
+    output entry, on a small periodic batch."""
+    rng = np.random.default_rng(5)
+    out = rng.normal(size=(2, 4, 5, 16))
+    tgt = rng.normal(size=(2, 4, 5, 16))
+    cx, cy = 0.5, 0.7
+    _, g = C.curl_loss_and_grad(out, tgt, cx, cy)
+    h = 1e-6
+    it = np.nditer(out, flags=["multi_index"])
+    for _ in it:
+        idx = it.multi_index
+        p = out.copy()
+        m = out.copy()
+        p[idx] += h
+        m[idx] -= h
+        fd = (C.curl_loss_and_grad(p, tgt, cx, cy)[0] - C.curl_loss_and_grad(m, tgt, cx, cy)[0]) / (2 * h)
+        assert abs(fd - g[idx]) < 1e-7, (idx, fd, g[idx])
+    # Channels outside the loss get no gradient.
+    assert np.all(g[..., 8:] == 0)
+
+
+def test_curl_of_a_potential_has_no_central_difference_divergence():
+    """The field correction dBx = dA/dy, dBy = -dA/dx (central differences,
+    periodic) leaves the central-difference div B unchanged: the property the
+    corrected run relies on."""
+    rng = np.random.default_rng(6)
+    A = rng.normal(size=(1, 8, 9))
+    dx, dy = 0.3, 0.2
+    dbx = (np.roll(A, -1, axis=1) - np.roll(A, 1, axis=1)) / (2 * dy)
+    dby = -(np.roll(A, -1, axis=2) - np.roll(A, 1, axis=2)) / (2 * dx)
+    div = (np.roll(dbx, -1, axis=2) - np.roll(dbx, 1, axis=2)) / (2 * dx) + \
+          (np.roll(dby, -1, axis=1) - np.roll(dby, 1, axis=1)) / (2 * dy)
+    assert np.abs(div).max() < 1e-12 * np.abs(A).max() / (dx * dy)
+
+
+def test_four_layer_network_with_curl_loss_matches_finite_differences():
+    rng = np.random.default_rng(7)
+    widths = [3, 4, 4, 4, 16]
+    params = [(rng.normal(0, 0.3, (co, 9, ci)), rng.normal(0, 0.1, co)) for ci, co in zip(widths[:-1], widths[1:])]
+    x = rng.normal(size=(1, 4, 5, 3))
+    tgt = rng.normal(size=(1, 4, 5, 16))
+    _, grads = C.net_curl_loss_and_grads(x, params, tgt, 0.5, 0.5)
+    h = 1e-6
+    for li in (0, 3):
+        W, b = params[li]
+        for idx in [(0, 4, 0), (2, 7, 1), (3, 0, 2)] if li == 0 else [(0, 4, 0), (5, 7, 1), (8, 0, 2)]:
+            Wp, Wm = W.copy(), W.copy()
+            Wp[idx] += h
+            Wm[idx] -= h
+            pp = list(params)
+            pm = list(params)
+            pp[li] = (Wp, b)
+            pm[li] = (Wm, b)
+            fd = (C.net_curl_loss_and_grads(x, pp, tgt, 0.5, 0.5)[0] -
+                  C.net_curl_loss_and_grads(x, pm, tgt, 0.5, 0.5)[0]) / (2 * h)
+            assert abs(fd - grads[li][0][idx]) < 1e-6 * max(1.0, abs(fd)), (li, idx, fd, grads[li][0][idx])
