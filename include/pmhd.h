@@ -316,6 +316,9 @@ typedef struct {
   int max_pairs;              /* capacity of the pair store (512)                */
   unsigned long long seed;    /* weight initialisation and minibatch order       */
   double div_tol;             /* allowed relative growth of ||div B||_1 (0.5)    */
+  double relax;               /* fraction of the predicted correction applied (1) */
+  double train_noise;         /* std of Gaussian noise added to the normalised
+                                 network inputs in training (0: none)          */
 } pmhd_learned_config;
 
 typedef struct {
@@ -345,6 +348,14 @@ int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, in
  * restricted fine state at the same time as its target. */
 int pmhd_learned_generate_rollout(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
                                   int every, int* added);
+/* As pmhd_learned_generate_rollout, but the coarse run is corrected by the
+ * current network (as in pmhd_learned_run) after every step: pairs along the
+ * trajectory the trained correction itself produces, each with the
+ * restricted fine state at the same time as its target (data aggregation
+ * against the correction's own compounding error).  Needs a trained network
+ * (PMHD_ERR_ARG otherwise). */
+int pmhd_learned_generate_corrected(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
+                                    int every, int* added);
 int pmhd_learned_num_pairs(const pmhd_learned* L);
 
 /* `iters` Adam steps (cosine decay from lr) on minibatches of `batch` pairs

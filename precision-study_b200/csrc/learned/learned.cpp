@@ -134,6 +134,62 @@ int check_err(pmhd_learned* L, cudaStream_t s) {
   return h ? PMHD_ERR_TIMEOUT : PMHD_OK;
 }
 
+// Device buffers of the per-step correction of one coarse grid.
+struct CorrBuffers {
+  CorrState cs{};
+  std::vector<void*> owned;
+  // plane: elements per SoA plane of the coarse solver; pix = nx * ny.
+  int alloc(const pmhd_learned* L, long long plane, long long pix, cudaStream_t s) {
+    auto grab = [&](cudaError_t e, void* p) {
+      owned.push_back(p);
+      return e == cudaSuccess;
+    };
+    bool ok = grab(dalloc(&cs.before, (size_t)kNVar * plane), cs.before);
+    ok = ok && grab(dalloc(&cs.cand, (size_t)pix * kNVar), cs.cand);
+    ok = ok && grab(dalloc(&cs.x, (size_t)pix * kFeat), cs.x) && grab(dalloc(&cs.z1, (size_t)pix * kWidth), cs.z1);
+    ok = ok && grab(dalloc(&cs.a1, (size_t)pix * kWidth), cs.a1) && grab(dalloc(&cs.z2, (size_t)pix * kWidth), cs.z2);
+    ok = ok && grab(dalloc(&cs.a2, (size_t)pix * kWidth), cs.a2) && grab(dalloc(&cs.out, (size_t)pix * kOut), cs.out);
+    ok = ok && grab(dalloc(&cs.z3, (size_t)pix * kWidth), cs.z3) && grab(dalloc(&cs.a3, (size_t)pix * kWidth), cs.a3);
+    ok = ok && grab(dalloc(&cs.flags, 4), cs.flags) && grab(dalloc(&cs.sums, 4), cs.sums);
+    ok = ok && grab(dalloc(&cs.counters, 4), cs.counters) && grab(dalloc(&cs.accept, 4), cs.accept);
+    if (!ok) {
+      cudaGetLastError();
+      return PMHD_ERR_NOMEM;
+    }
+    cs.norm = L->dnorm;
+    cs.relax = L->cfg.relax;
+    cudaError_t e = cudaMemsetAsync(cs.flags, 0, 4 * sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cs.sums, 0, 4 * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cs.counters, 0, 4 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? PMHD_OK : PMHD_ERR_CUDA;
+  }
+  ~CorrBuffers() {
+    for (void* p : owned)
+      if (p) cudaFree(p);
+  }
+};
+
+// The network on one coarse grid: features of (u after the step, the state
+// before it) -> four convolutions -> cs.out.
+cudaError_t net_infer(const NetLayout& N, const NetWeights& W, const CorrState& cs, const void* u, int pitch,
+                      long long plane, int nx, int ny, int* err, cudaStream_t s) {
+  cudaError_t r = features(soa_view(u, pitch, plane), soa_view(cs.before, pitch, plane), 1, nx, ny, cs.norm, cs.x, s);
+  if (r == cudaSuccess)
+    r = conv3x3(CONV_GELU, cs.x, 1, ny, nx, kFeat, W.wf[0], W.theta + N.b_off[0], kWidth, nullptr, cs.z1, cs.a1, err,
+                s);
+  if (r == cudaSuccess)
+    r = conv3x3(CONV_GELU, cs.a1, 1, ny, nx, kWidth, W.wf[1], W.theta + N.b_off[1], kWidth, nullptr, cs.z2, cs.a2, err,
+                s);
+  if (r == cudaSuccess)
+    r = conv3x3(CONV_GELU, cs.a2, 1, ny, nx, kWidth, W.wf[2], W.theta + N.b_off[2], kWidth, nullptr, cs.z3, cs.a3, err,
+                s);
+  if (r == cudaSuccess)
+    r = conv3x3(CONV_LINEAR, cs.a3, 1, ny, nx, kWidth, W.wf[3], W.theta + N.b_off[3], kOut, nullptr, cs.out, nullptr,
+                err, s);
+  return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -155,6 +211,8 @@ int pmhd_learned_config_default(pmhd_learned_config* c) {
   c->max_pairs = 512;
   c->seed = 1;
   c->div_tol = 0.5;
+  c->relax = 1.0;
+  c->train_noise = 0.0;
   return PMHD_OK;
 }
 
@@ -179,7 +237,8 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
   *out = nullptr;
   if (!cfg || cfg->nx < 8 || cfg->ny < 8 || cfg->refine < 2 || cfg->refine > 16 || cfg->max_pairs < 1 ||
       !(cfg->x_max > cfg->x_min) || !(cfg->y_max > cfg->y_min) || !(cfg->gamma > 1.0) || !(cfg->cfl > 0.0) ||
-      !(cfg->cfl < 1.0) || !(cfg->alpha > 0.0) || !(cfg->div_tol >= 0.0))
+      !(cfg->cfl < 1.0) || !(cfg->alpha > 0.0) || !(cfg->div_tol >= 0.0) ||
+      !(cfg->relax >= 0.0) || !(cfg->relax <= 1.0) || !(cfg->train_noise >= 0.0))
     return PMHD_ERR_ARG;
   if (cfg->precision != PMHD_FP64 && cfg->precision != PMHD_MIXED) return PMHD_ERR_UNSUPPORTED;
   int ndev = 0;
@@ -259,14 +318,20 @@ int pmhd_learned_num_pairs(const pmhd_learned* L) { return L ? L->npairs : 0; }
 namespace {
 
 // Training pairs (before, plain coarse step, restricted fine state at the
-// same time) along a fine run.  rollout = false: every coarse step starts
-// from the restricted fine state; true: the coarse run keeps its own state
-// after the first step (the states a corrected run actually meets), and the
-// target stays the restricted fine state.
+// same time) along a fine run.  mode PAIRS_FINE: every coarse step starts
+// from the restricted fine state; PAIRS_ROLLOUT: the coarse run keeps its own
+// state after the first step (the plain coarse trajectory); PAIRS_CORRECTED:
+// the coarse run is corrected by the current network after every step (the
+// states a corrected run meets, DAgger-style data aggregation).  The target
+// is always the restricted fine state at the same time.
+enum PairMode { PAIRS_FINE = 0, PAIRS_ROLLOUT = 1, PAIRS_CORRECTED = 2 };
+
 int generate_pairs(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
-                   int* added, bool rollout) {
+                   int* added, int mode) {
   if (added) *added = 0;
   if (!L || every < 1 || !(t_end > 0.0)) return PMHD_ERR_ARG;
+  if (mode == PAIRS_CORRECTED && !L->have_norm) return PMHD_ERR_ARG;  // needs a trained network
+  const bool rollout = mode != PAIRS_FINE;
   L_CU(cudaSetDevice(L->cfg.device));
   const int r = L->cfg.refine;
   const pmhd_config fc = solver_config(L->cfg, r), cc = solver_config(L->cfg, 1);
@@ -278,6 +343,12 @@ int generate_pairs(pmhd_learned* L, int problem, const double* params, int npara
   SolverView vf, vc;
   solver_view(f.s, &vf);
   solver_view(c.s, &vc);
+  CorrBuffers cb;
+  if (mode == PAIRS_CORRECTED) {
+    rc = cb.alloc(L, vc.plane, (long long)vc.nx * vc.ny, vc.stream);
+    if (rc != PMHD_OK) return rc;
+  }
+  const size_t state_bytes = (size_t)kNVar * vc.plane * sizeof(double);
   double *cur = nullptr, *nxt = nullptr, *yy = nullptr;
   if (dalloc(&cur, L->pair_elems) != cudaSuccess || dalloc(&nxt, L->pair_elems) != cudaSuccess ||
       dalloc(&yy, L->pair_elems) != cudaSuccess) {
@@ -298,6 +369,8 @@ int generate_pairs(pmhd_learned* L, int problem, const double* params, int npara
     } else {
       e = store_interior(vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, cur, vc.stream);
     }
+    if (e == cudaSuccess && mode == PAIRS_CORRECTED)
+      e = cudaMemcpyAsync(cb.cs.before, vc.u, state_bytes, cudaMemcpyDeviceToDevice, vc.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(vc.stream);
     if (e != cudaSuccess) break;
     pmhd_set_time(c.s, t, 0);
@@ -322,6 +395,16 @@ int generate_pairs(pmhd_learned* L, int problem, const double* params, int npara
       L->npairs++;
       n_added++;
     }
+    if (mode == PAIRS_CORRECTED) {
+      // The network's correction of this step, applied in place to the
+      // coarse state the next iteration starts from (checked as in a run).
+      e = net_infer(L->L, L->w, cb.cs, vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, L->err, vc.stream);
+      if (e == cudaSuccess)
+        e = correct_step(cb.cs, vc.u, vc.pitch, vc.plane, vc.nx, vc.ny, vc.dx, vc.dy, vc.gamma, L->cfg.div_tol,
+                         nullptr, nullptr, 0, vc.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(vc.stream);
+      if (e != cudaSuccess) break;
+    }
     double* tmp = cur;
     cur = nxt;
     nxt = tmp;
@@ -345,12 +428,17 @@ extern "C" {
 
 int pmhd_learned_generate(pmhd_learned* L, int problem, const double* params, int nparams, double t_end, int every,
                           int* added) {
-  return generate_pairs(L, problem, params, nparams, t_end, every, added, false);
+  return generate_pairs(L, problem, params, nparams, t_end, every, added, PAIRS_FINE);
 }
 
 int pmhd_learned_generate_rollout(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
                                   int every, int* added) {
-  return generate_pairs(L, problem, params, nparams, t_end, every, added, true);
+  return generate_pairs(L, problem, params, nparams, t_end, every, added, PAIRS_ROLLOUT);
+}
+
+int pmhd_learned_generate_corrected(pmhd_learned* L, int problem, const double* params, int nparams, double t_end,
+                                    int every, int* added) {
+  return generate_pairs(L, problem, params, nparams, t_end, every, added, PAIRS_CORRECTED);
 }
 
 int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* losses) {
@@ -448,6 +536,8 @@ int pmhd_learned_train(pmhd_learned* L, int iters, int batch, double lr, float* 
   float* g = L->grad;
   auto iteration = [&]() -> cudaError_t {
     cudaError_t r = gather_pairs(sched, it, batch, feat_all, tgt_all, pix, xb, tb, s);
+    if (r == cudaSuccess && L->cfg.train_noise > 0.0)
+      r = input_noise(xb, P, (float)L->cfg.train_noise, it, L->cfg.seed, s);
     if (r == cudaSuccess)
       r = conv3x3(CONV_GELU, xb, batch, ny, nx, kFeat, L->w.wf[0], th + N.b_off[0], kWidth, nullptr, z1, a1, L->err, s);
     if (r == cudaSuccess)
@@ -514,44 +604,16 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
   solver_view(c.s, &vc);
   const int nx = vc.nx, ny = vc.ny;
   const long long pix = (long long)nx * ny;
-  CorrState cs{};
-  std::vector<void*> owned;
-  auto grab = [&](cudaError_t e, void* p) {
-    owned.push_back(p);
-    return e == cudaSuccess;
-  };
-  bool ok = grab(dalloc(&cs.before, (size_t)kNVar * vc.plane), cs.before);
-  ok = ok && grab(dalloc(&cs.cand, (size_t)pix * kNVar), cs.cand);
-  ok = ok && grab(dalloc(&cs.x, (size_t)pix * kFeat), cs.x) && grab(dalloc(&cs.z1, (size_t)pix * kWidth), cs.z1);
-  ok = ok && grab(dalloc(&cs.a1, (size_t)pix * kWidth), cs.a1) && grab(dalloc(&cs.z2, (size_t)pix * kWidth), cs.z2);
-  ok = ok && grab(dalloc(&cs.a2, (size_t)pix * kWidth), cs.a2) && grab(dalloc(&cs.out, (size_t)pix * kOut), cs.out);
-  ok = ok && grab(dalloc(&cs.z3, (size_t)pix * kWidth), cs.z3) && grab(dalloc(&cs.a3, (size_t)pix * kWidth), cs.a3);
-  ok = ok && grab(dalloc(&cs.flags, 4), cs.flags) && grab(dalloc(&cs.sums, 4), cs.sums);
-  ok = ok && grab(dalloc(&cs.counters, 4), cs.counters) && grab(dalloc(&cs.accept, 4), cs.accept);
-  auto release = [&]() {
-    for (void* p : owned)
-      if (p) cudaFree(p);
-  };
-  if (!ok) {
-    cudaGetLastError();
-    release();
-    return PMHD_ERR_NOMEM;
-  }
-  cs.norm = L->dnorm;
-  cudaError_t e = cudaMemsetAsync(cs.flags, 0, 4 * sizeof(int), vc.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(cs.sums, 0, 4 * sizeof(double), vc.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(cs.counters, 0, 4 * sizeof(unsigned long long), vc.stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(L->err, 0, sizeof(int), vc.stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(vc.stream);
-  if (e != cudaSuccess) {
-    release();
+  CorrBuffers cb;
+  rc = cb.alloc(L, vc.plane, pix, vc.stream);
+  if (rc != PMHD_OK) return rc;
+  const CorrState cs = cb.cs;
+  if (cudaMemsetAsync(L->err, 0, sizeof(int), vc.stream) != cudaSuccess ||
+      cudaStreamSynchronize(vc.stream) != cudaSuccess)
     return PMHD_ERR_CUDA;
-  }
   rc = load_restricted_ic(L, c.s, problem, params, nparams, cs.cand);
-  if (rc != PMHD_OK) {
-    release();
-    return rc;
-  }
+  if (rc != PMHD_OK) return rc;
+  cudaError_t e = cudaSuccess;
   if (use_net) {
     const NetLayout N = L->L;
     const NetWeights W = L->w;
@@ -563,20 +625,7 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
     };
     auto post = [=](int p) -> cudaError_t {
       cudaStream_t s = vc.stream;
-      cudaError_t r = features(soa_view(vc.u, vc.pitch, vc.plane), soa_view(cs.before, vc.pitch, vc.plane), 1, nx, ny,
-                               cs.norm, cs.x, s);
-      if (r == cudaSuccess)
-        r = conv3x3(CONV_GELU, cs.x, 1, ny, nx, kFeat, W.wf[0], W.theta + N.b_off[0], kWidth, nullptr, cs.z1, cs.a1,
-                    err, s);
-      if (r == cudaSuccess)
-        r = conv3x3(CONV_GELU, cs.a1, 1, ny, nx, kWidth, W.wf[1], W.theta + N.b_off[1], kWidth, nullptr, cs.z2, cs.a2,
-                    err, s);
-      if (r == cudaSuccess)
-        r = conv3x3(CONV_GELU, cs.a2, 1, ny, nx, kWidth, W.wf[2], W.theta + N.b_off[2], kWidth, nullptr, cs.z3, cs.a3,
-                    err, s);
-      if (r == cudaSuccess)
-        r = conv3x3(CONV_LINEAR, cs.a3, 1, ny, nx, kWidth, W.wf[3], W.theta + N.b_off[3], kOut, nullptr, cs.out,
-                    nullptr, err, s);
+      cudaError_t r = net_infer(N, W, cs, vc.u, vc.pitch, vc.plane, nx, ny, err, s);
       if (r == cudaSuccess)
         r = correct_step(cs, vc.u, vc.pitch, vc.plane, nx, ny, vc.dx, vc.dy, vc.gamma, div_tol, vc.ctrl, vc.ctrl, p, s);
       if (r == cudaSuccess)
@@ -608,7 +657,6 @@ int pmhd_learned_run(pmhd_learned* L, int problem, const double* params, int npa
   }
   if (use_net) solver_set_step_hooks(c.s, nullptr, nullptr);
   if (rc == PMHD_OK) rc = check_err(L, vc.stream);
-  release();
   return rc;
 }
 

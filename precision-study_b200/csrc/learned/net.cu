@@ -36,8 +36,10 @@ __device__ __forceinline__ double sv(const StateView& s, long long b, int k, int
   return s.u[s.offset + b * s.bstride + k * s.vstride + j * s.jstride + i * s.istride];
 }
 
-// Whether the step of parity p was taken and left a usable state.
+// Whether the step of parity p was taken and left a usable state (no
+// control block: a correction applied outside a solver step, always).
 __device__ __forceinline__ bool step_taken(const Ctrl* c, int p) {
+  if (c == nullptr) return true;
   return c->step[p ^ 1] != c->step[p] && !c->halted && !c->err && c->bad1 == BAD_NONE && c->bad2 == BAD_NONE;
 }
 
@@ -273,6 +275,28 @@ __global__ void gather_kernel(const int* __restrict__ schedule, const int* __res
 
 __global__ void increment_kernel(int* it) { *it += 1; }
 
+// splitmix64 finaliser as a counter-based hash (published mixing constants).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void input_noise_kernel(__nv_bfloat16* __restrict__ x, long long n, float sigma,
+                                   const int* __restrict__ it, unsigned long long seed) {
+  const unsigned long long base = mix64(seed ^ (0x9e3779b97f4a7c15ull * (unsigned long long)(*it + 1)));
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long q = e / (2 * kNVar), c = e % (2 * kNVar);
+    const unsigned long long h = mix64(base + (unsigned long long)e);
+    // Box-Muller from two 24-bit uniforms in (0, 1).
+    const float u1 = ((float)(h >> 40) + 0.5f) * (1.0f / 16777216.0f);
+    const float u2 = ((float)((h >> 16) & 0xFFFFFF) + 0.5f) * (1.0f / 16777216.0f);
+    const float g = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+    __nv_bfloat16* p = x + q * kFeat + c;
+    *p = __float2bfloat16_rn(__bfloat162float(*p) + sigma * g);
+  }
+}
+
 __global__ void restrict_kernel(const double* __restrict__ fu, int fpitch, long long fplane, int fnx, int r,
                                 int nx, int ny, double* __restrict__ coarse) {
   const long long n = (long long)nx * ny * kNVar;
@@ -317,19 +341,19 @@ __global__ void store_interior_kernel(const double* __restrict__ u, int pitch, l
 // density or pressure is not positive (or not finite).
 __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long long plane, int nx, int ny,
                                  const float* __restrict__ out, const Norm* __restrict__ norm, double gamma,
-                                 double dx, double dy, double* __restrict__ cand, int* __restrict__ flags,
-                                 const Ctrl* __restrict__ c, int p) {
+                                 double dx, double dy, double relax, double* __restrict__ cand,
+                                 int* __restrict__ flags, const Ctrl* __restrict__ c, int p) {
   if (!step_taken(c, p)) return;
   const long long n = (long long)nx * ny;
   int bad = 0;
-  const double sA = norm->sig_out[OUT_A];
+  const double sA = relax * norm->sig_out[OUT_A];
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx), j = (int)(q / nx);
     double U[kNVar];
 #pragma unroll
     for (int k = 0; k < kNVar; k++) U[k] = u[k * plane + (long long)(j + 2) * pitch + (i + 2)];
     const float* o = out + q * kOut;
-    auto sig = [&](int k) { return (double)norm->sig_out[k] * (double)o[k]; };
+    auto sig = [&](int k) { return relax * (double)norm->sig_out[k] * (double)o[k]; };
     auto clamp2 = [](double x) { return x < -2.0 ? -2.0 : (x > 2.0 ? 2.0 : x); };
     const double rho = U[0], inv = 1.0 / rho;
     const double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
@@ -400,7 +424,7 @@ __global__ void decide_kernel(int* __restrict__ flags, double* __restrict__ sums
     } else {
       counters[0]++;
       acc = 1;
-      c->chbits[p ^ 1] = 0ull;  // the next step's speed is recomputed from the corrected state
+      if (c) c->chbits[p ^ 1] = 0ull;  // the next step's speed is recomputed from the corrected state
     }
   }
   *accept = acc;
@@ -482,6 +506,13 @@ cudaError_t increment(int* it, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t input_noise(__nv_bfloat16* x, long long P, float sigma, const int* it, unsigned long long seed,
+                        cudaStream_t s) {
+  const long long n = P * 2 * kNVar;
+  input_noise_kernel<<<grid_for(n, 256), 256, 0, s>>>(x, n, sigma, it, seed);
+  return cudaGetLastError();
+}
+
 cudaError_t restrict_state(const void* fine_u, int fpitch, long long fplane, int fnx, int fny, int r, double* coarse,
                            cudaStream_t s) {
   const int nx = fnx / r, ny = fny / r;
@@ -508,7 +539,7 @@ cudaError_t correct_step(const CorrState& cs, void* u, int pitch, long long plan
   double* ud = static_cast<double*>(u);
   const long long n = (long long)nx * ny;
   candidate_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.out, cs.norm, gamma, dx, dy,
-                                                    cs.cand, cs.flags, ctrl, p);
+                                                    cs.relax, cs.cand, cs.flags, ctrl, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   divnorm_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.cand, dx, dy, cs.sums, ctrl, p);

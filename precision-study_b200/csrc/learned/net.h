@@ -86,6 +86,7 @@ struct CorrState {
   unsigned long long* counters;
   int* accept;
   const Norm* norm;    // device copy
+  double relax;        // fraction of the predicted correction applied
 };
 
 cudaError_t features(const StateView& after, const StateView& before, int batch, int nx, int ny, const Norm* norm,
@@ -111,6 +112,10 @@ cudaError_t gather_pairs(const int* schedule, const int* it, int batch, const __
                          const float* tgt_all, long long pix_per_pair, __nv_bfloat16* feat, float* tgt,
                          cudaStream_t s);
 cudaError_t increment(int* it, cudaStream_t s);
+// Adds N(0, sigma^2) to the used input channels (0 .. 2 * kNVar - 1) of P
+// pixels of a feature batch; the draws depend on (seed, *it, element).
+cudaError_t input_noise(__nv_bfloat16* x, long long P, float sigma, const int* it, unsigned long long seed,
+                        cudaStream_t s);
 // Block average of a fine SoA state (factor r) into a coarse AoS interior.
 cudaError_t restrict_state(const void* fine_u, int fpitch, long long fplane, int fnx, int fny, int r, double* coarse,
                            cudaStream_t s);

@@ -43,7 +43,7 @@ EXPORTS = (
     "pmhd_ensemble_member_stats", "pmhd_ensemble_get_state", "pmhd_ensemble_destroy",
     "pmhd_conv3x3", "pmhd_conv3x3_wgrad", "pmhd_learned_loss_grad",
     "pmhd_learned_config_default", "pmhd_learned_create", "pmhd_learned_destroy", "pmhd_learned_generate",
-    "pmhd_learned_generate_rollout",
+    "pmhd_learned_generate_rollout", "pmhd_learned_generate_corrected",
     "pmhd_learned_num_pairs", "pmhd_learned_train", "pmhd_learned_run", "pmhd_learned_fine_run",
     "pmhd_learned_save", "pmhd_learned_load",
     "pmhd_euler2d_create", "pmhd_euler2d_advance", "pmhd_euler2d_get_prim", "pmhd_euler2d_destroy",
@@ -113,7 +113,8 @@ class LearnedConfig(ctypes.Structure):
         ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
         ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("alpha", ctypes.c_double),
         ("precision", ctypes.c_int), ("device", ctypes.c_int), ("max_pairs", ctypes.c_int),
-        ("seed", ctypes.c_ulonglong), ("div_tol", ctypes.c_double),
+        ("seed", ctypes.c_ulonglong), ("div_tol", ctypes.c_double), ("relax", ctypes.c_double),
+        ("train_noise", ctypes.c_double),
     ]
 
 
@@ -178,6 +179,7 @@ def load():
         "pmhd_learned_destroy": ([vp], i),
         "pmhd_learned_generate": ([vp, i, P(d), i, d, i, P(i)], i),
         "pmhd_learned_generate_rollout": ([vp, i, P(d), i, d, i, P(i)], i),
+        "pmhd_learned_generate_corrected": ([vp, i, P(d), i, d, i, P(i)], i),
         "pmhd_learned_num_pairs": ([vp], i),
         "pmhd_learned_train": ([vp, i, i, d, P(ctypes.c_float)], i),
         "pmhd_learned_run": ([vp, i, P(d), i, d, i, P(d), P(LearnedStats)], i),
@@ -473,12 +475,15 @@ class Learned:
     def num_pairs(self):
         return load().pmhd_learned_num_pairs(self._h)
 
-    def generate(self, problem=PROBLEM_ORSZAG_TANG, params=None, t_end=0.5, every=1, rollout=False):
+    def generate(self, problem=PROBLEM_ORSZAG_TANG, params=None, t_end=0.5, every=1, rollout=False,
+                 corrected=False):
         """Training pairs; rollout=True takes them along the plain coarse
-        trajectory (pmhd_learned_generate_rollout)."""
+        trajectory (pmhd_learned_generate_rollout), corrected=True along the
+        trajectory the current network corrects (pmhd_learned_generate_corrected)."""
         arr, n = _params_arg(params)
         added = ctypes.c_int()
-        fn = "pmhd_learned_generate_rollout" if rollout else "pmhd_learned_generate"
+        fn = ("pmhd_learned_generate_corrected" if corrected else
+              "pmhd_learned_generate_rollout" if rollout else "pmhd_learned_generate")
         _check(getattr(load(), fn)(self._h, problem, arr, n, t_end, every, ctypes.byref(added)), fn)
         return added.value
 
