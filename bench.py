@@ -452,50 +452,66 @@ def bench_euler(pmhd, n, W, K, device, max_over_ranks, world):
     return out
 
 
-def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=2, max_pairs=640, seed=11):
-    """Learned correction of the Orszag-Tang family (field scaled by B0):
-    training pairs from four amplitudes on the n^2 coarse / (refine n)^2 fine
-    grids, evaluation on the held-out B0 = 1.  Errors are relative L2 (mean
-    over the non-trivial variables, and rho) against the fine run restricted
-    to the coarse grid; wall times are those of the time loops."""
+def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, max_pairs=1500, seed=11,
+                  kh=False, precision="mixed"):
+    """Learned correction: training pairs from the solver (Orszag-Tang with
+    the field scaled by B0 in {0.7, 0.85, 1.15, 1.3}; with kh, also the
+    periodic Kelvin-Helmholtz double shear layer with widths {0.03, 0.045,
+    0.065, 0.08}) on the n^2 coarse / (refine n)^2 fine grids, evaluation on
+    the held-out B0 = 1 (and width 0.055).  Errors are relative L2 (rho, the
+    mean over rho, mx, my, E, Bx, By, and all values at once) against the fine
+    run restricted to the coarse grid; wall times are those of the time
+    loops; the corrected run's speed-up is against the fine run's wall."""
     import numpy as np
-    OT = pmhd.PROBLEM_ORSZAG_TANG
-    live = [0, 1, 2, 4, 5, 6, 8]  # rho, mx, my, E, Bx, By, psi (mz = Bz = 0 in 2D OT)
+    OT, KH = pmhd.PROBLEM_ORSZAG_TANG, pmhd.PROBLEM_KH_REF
+    live = [0, 1, 2, 4, 5, 6]
 
     def err(a, ref):
         r = pmhd.relative_l2(ref, a)
         whole = float(np.sqrt(np.mean((a - ref) ** 2)) / np.sqrt(np.mean(ref ** 2)))  # all values at once
-        return {"rho": float(r[0]), "mean": float(np.mean([r[k] for k in live if k != 8])), "all": whole}
+        return {"rho": float(r[0]), "mean": float(np.mean([r[k] for k in live])), "all": whole}
 
-    out = {"coarse": n, "fine": refine * n, "problem": "Orszag-Tang, B0 in {0.7,0.85,1.15,1.3} train, B0=1 test",
-           "t_end": t_end, "pairs_every": every}
-    with pmhd.Learned(nx=n, ny=n, refine=refine, max_pairs=max_pairs, seed=seed, device=device) as L:
+    train = [(OT, [b]) for b in (0.7, 0.85, 1.15, 1.3)]
+    tests = {"orszag_tang_B0_1": (OT, [1.0])}
+    if kh:
+        train += [(KH, [w]) for w in (0.03, 0.045, 0.065, 0.08)]
+        tests["kh_width_0.055"] = (KH, [0.055])
+    out = {"coarse": n, "fine": refine * n, "precision": precision, "t_end": t_end, "pairs_every": every,
+           "train": ("Orszag-Tang B0 in {0.7,0.85,1.15,1.3}" +
+                     (" + periodic KH width in {0.03,0.045,0.065,0.08}" if kh else "")),
+           "network": "4 x 3x3 conv, 32 channels, GELU, bf16 tcgen05, fp32 accumulation"}
+    with pmhd.Learned(nx=n, ny=n, refine=refine, max_pairs=max_pairs, seed=seed, device=device,
+                      precision=precision) as L:
+        out["relax"], out["train_noise"] = L.cfg.relax, L.cfg.train_noise
         t0 = time.perf_counter()
-        for b0 in (0.7, 0.85, 1.15, 1.3):
-            L.generate(OT, [b0], t_end=t_end, every=every)
+        for prob, par in train:
+            L.generate(prob, par, t_end=t_end, every=every)
         t1 = time.perf_counter()
         losses = L.train(iters=iters, batch=8, lr=2e-3)
         t2 = time.perf_counter()
-        fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=refine)
-        plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
-        two, s2 = L.fine_run(OT, [1.0], t_end=t_end, refine=2)
-        try:
-            corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
-        except pmhd.PmhdError as exc:  # a corrected state the solver could not advance
-            out.update({"pairs": L.num_pairs, "corrected_run": f"failed: {exc}"})
-            return out
-        out.update({
-            "pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": iters,
-            "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-100:].mean()),
-            "relL2_vs_fine": {"plain_coarse": err(plain, fine), "learned_coarse": err(corr, fine),
-                              "plain_2x": err(two, fine)},
-            "wall_ms": {"fine": sf.wall_ms, "plain_coarse": sp.wall_ms, "learned_coarse": sc.wall_ms,
-                        "plain_2x": s2.wall_ms},
-            "steps": {"fine": sf.steps, "plain_coarse": sp.steps, "learned_coarse": sc.steps, "plain_2x": s2.steps},
-            "corrections": {"accepted": sc.accepted, "rejected_positivity": sc.rejected_positivity,
-                            "rejected_divergence": sc.rejected_divergence},
-            "speedup_vs_fine_wall": sf.wall_ms / sc.wall_ms,
-        })
+        out.update({"pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": iters,
+                    "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-100:].mean())})
+        for name, (prob, par) in tests.items():
+            fine, sf = L.fine_run(prob, par, t_end=t_end, refine=refine)
+            plain, sp = L.run(prob, par, t_end=t_end, use_net=False)
+            two, s2 = L.fine_run(prob, par, t_end=t_end, refine=2)
+            rec = {}
+            try:
+                corr, sc = L.run(prob, par, t_end=t_end, use_net=True)
+            except pmhd.PmhdError as exc:  # a corrected state the solver could not advance
+                rec["corrected_run"] = f"failed: {exc}"
+                corr, sc = None, None
+            rec["relL2_vs_fine"] = {"plain_coarse": err(plain, fine), "plain_2x": err(two, fine)}
+            rec["wall_ms"] = {"fine": sf.wall_ms, "plain_coarse": sp.wall_ms, "plain_2x": s2.wall_ms}
+            if corr is not None:
+                rec["relL2_vs_fine"]["learned_coarse"] = err(corr, fine)
+                rec["wall_ms"]["learned_coarse"] = sc.wall_ms
+                rec["corrections"] = {"accepted": sc.accepted, "rejected_positivity": sc.rejected_positivity,
+                                      "rejected_divergence": sc.rejected_divergence, "steps": sc.steps}
+                rec["speedup_vs_fine_wall"] = sf.wall_ms / sc.wall_ms
+                rec["gain"] = {k: rec["relL2_vs_fine"]["learned_coarse"][k] < rec["relL2_vs_fine"]["plain_coarse"][k]
+                               for k in ("rho", "mean", "all")}
+            out[name] = rec
     return out
 
 
@@ -555,7 +571,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
     ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
     ap.add_argument("--ensemble-seed", type=int, default=20261203)
-    ap.add_argument("--learned", type=int, default=128, help="coarse grid of the learned-correction line (0: skip)")
+    ap.add_argument("--learned", type=int, default=512, help="coarse grid of the learned-correction line (0: skip)")
     ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
     ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
     ap.add_argument("--hancock", type=int, default=4096, help="grid of the MUSCL-Hancock line (0: skip)")
@@ -683,11 +699,14 @@ def main():
     # ---- learned coarse-grid correction: accuracy and wall time ---------------
     learned = None
     if args.learned > 0 and rank == 0:
-        # The coarse grid where the correction gains (the GPU test's case), then
-        # the larger one where it does not.
-        learned = {"coarse_32": bench_learned(pmhd, 32, local, t_end=0.2, iters=args.learned_iters, every=1,
-                                              max_pairs=600, seed=7),
-                   f"coarse_{args.learned}": bench_learned(pmhd, args.learned, local, iters=args.learned_iters)}
+        # The GPU test's case (64^2 coarse), then the larger configuration.
+        learned = {"coarse_64": bench_learned(pmhd, 64, local, iters=args.learned_iters)}
+        if args.learned >= 128:
+            # BASELINE's configuration: 2048^2 fine -> 512^2 coarse, OT and KH
+            # states, fine runs in binary64.
+            learned[f"coarse_{args.learned}"] = bench_learned(
+                pmhd, args.learned, local, iters=1000, every=max(1, args.learned // 32), max_pairs=600, kh=True,
+                precision="fp64")
 
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
     cpu = None

@@ -316,9 +316,11 @@ typedef struct {
   int max_pairs;              /* capacity of the pair store (512)                */
   unsigned long long seed;    /* weight initialisation and minibatch order       */
   double div_tol;             /* allowed relative growth of ||div B||_1 (0.5)    */
-  double relax;               /* fraction of the predicted correction applied (1) */
+  double relax;               /* fraction of the predicted correction applied
+                                 (0.25; the full correction compounds its error
+                                 into an unstable run)                         */
   double train_noise;         /* std of Gaussian noise added to the normalised
-                                 network inputs in training (0: none)          */
+                                 network inputs in training (0.03; 0: none)   */
 } pmhd_learned_config;
 
 typedef struct {

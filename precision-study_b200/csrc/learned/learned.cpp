@@ -211,8 +211,8 @@ int pmhd_learned_config_default(pmhd_learned_config* c) {
   c->max_pairs = 512;
   c->seed = 1;
   c->div_tol = 0.5;
-  c->relax = 1.0;
-  c->train_noise = 0.0;
+  c->relax = 0.25;
+  c->train_noise = 0.03;
   return PMHD_OK;
 }
 

@@ -244,37 +244,63 @@ def _rel(a, b):
     return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
 
 
+def _rel_rho_mean(a, ref):
+    """Relative L2 of rho and the mean over the six non-trivial conserved
+    variables (rho, mx, my, E, Bx, By), per-variable RMS(a - ref) / RMS(ref)."""
+    r = [float(np.sqrt(np.mean((a[..., k] - ref[..., k]) ** 2)) / np.sqrt(np.mean(ref[..., k] ** 2)))
+         for k in (0, 1, 2, 4, 5, 6)]
+    return r[0], float(np.mean(r))
+
+
 def test_learned_correction_trains_and_beats_the_plain_coarse_grid(pmhd_lib, tmp_path):
     """Orszag-Tang with the field scaled by B0: pairs from four training
-    amplitudes (coarse 32^2, fine 128^2), evaluation on a held-out amplitude.
-    The corrected coarse run must be closer to the restricted fine run than
-    the plain coarse run; every correction passes the checks or is counted."""
+    amplitudes (coarse 64^2, fine 256^2), evaluation on the held-out amplitude
+    B0 = 1 at t = 0.25.  Judged against the restricted fine run, the corrected
+    coarse run must beat the plain coarse run in rho AND in the mean over the
+    variables; every correction passes the checks or is counted."""
     OT = pmhd_lib.PROBLEM_ORSZAG_TANG
-    t_end = 0.2
-    with pmhd_lib.Learned(nx=32, ny=32, refine=4, max_pairs=600, seed=7) as L:
+    t_end = 0.25
+    with pmhd_lib.Learned(nx=64, ny=64, refine=4, max_pairs=1500, seed=11) as L:
+        assert L.cfg.relax == 0.25 and L.cfg.train_noise == 0.03  # the defaults
         for b0 in (0.7, 0.85, 1.15, 1.3):
-            assert L.generate(OT, [b0], t_end=t_end, every=1) > 10
+            assert L.generate(OT, [b0], t_end=t_end, every=1) > 100
         losses = L.train(iters=1500, batch=8, lr=2e-3)
         assert np.all(np.isfinite(losses))
-        assert losses[-100:].mean() < 0.5 * losses[:10].mean()
+        assert losses[-100:].mean() < 0.2 * losses[:10].mean()
         fine, sf = L.fine_run(OT, [1.0], t_end=t_end, refine=4)
         plain, sp = L.run(OT, [1.0], t_end=t_end, use_net=False)
         corr, sc = L.run(OT, [1.0], t_end=t_end, use_net=True)
-        assert sp.t == sc.t == t_end  # the corrected run's CFL steps differ slightly
+        assert sp.t == sc.t == t_end
         assert sc.accepted + sc.rejected_positivity + sc.rejected_divergence == sc.steps
-        assert sc.accepted > 0
-        e_plain, e_corr = _rel(plain, fine), _rel(corr, fine)
-        print(f"relL2 vs restricted fine: plain {e_plain:.3e} corrected {e_corr:.3e}; "
-              f"accepted {sc.accepted}/{sc.steps}; loss {losses[:10].mean():.3e} -> {losses[-100:].mean():.3e}")
-        assert e_corr < e_plain
+        assert sc.accepted > 0.9 * sc.steps  # positivity-safe outputs, curl field: few rejections
+        rho_p, mean_p = _rel_rho_mean(plain, fine)
+        rho_c, mean_c = _rel_rho_mean(corr, fine)
+        print(f"relL2 vs restricted fine: rho plain {rho_p:.4e} corrected {rho_c:.4e}; mean plain {mean_p:.4e} "
+              f"corrected {mean_c:.4e}; accepted {sc.accepted}/{sc.steps}")
+        assert rho_c < rho_p and mean_c < mean_p
         # Weights and normalisation survive a save / load into a new handle.
         path = str(tmp_path / "net.bin")
         L.save(path)
-        with pmhd_lib.Learned(nx=32, ny=32, refine=4, max_pairs=1, seed=99) as L2:
+        with pmhd_lib.Learned(nx=64, ny=64, refine=4, max_pairs=1, seed=99) as L2:
             L2.load_weights(path)
             corr2, sc2 = L2.run(OT, [1.0], t_end=t_end, use_net=True)
             assert sc2.steps == sc.steps
             np.testing.assert_allclose(corr2, corr, rtol=0, atol=1e-12 * np.abs(corr).max())
+
+
+def test_corrected_trajectory_pairs_need_a_trained_network(pmhd_lib):
+    """pmhd_learned_generate_corrected takes pairs along the run the current
+    network corrects: refused before training, one pair per coarse step
+    after it."""
+    OT = pmhd_lib.PROBLEM_ORSZAG_TANG
+    with pmhd_lib.Learned(nx=32, ny=32, refine=2, max_pairs=400, seed=5) as L:
+        with pytest.raises(pmhd_lib.PmhdError) as e:
+            L.generate(OT, [1.0], t_end=0.05, corrected=True)
+        assert e.value.status == pmhd_lib.ERR_ARG
+        n0 = L.generate(OT, [1.0], t_end=0.05)
+        L.train(iters=100, batch=4, lr=1e-3)
+        n1 = L.generate(OT, [1.0], t_end=0.05, corrected=True)
+        assert n0 > 5 and abs(n1 - n0) <= 2 and L.num_pairs == n0 + n1
 
 
 def test_rollout_pairs_follow_the_coarse_trajectory(pmhd_lib):
