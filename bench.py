@@ -452,6 +452,64 @@ def bench_euler(pmhd, n, W, K, device, max_over_ranks, world):
     return out
 
 
+# Published A30 times of the reference's shock-bubble GPU program (src/euler/euler2d_cuda.cu,
+# 500 x 197, 3459 steps to t = 0.0011741 s): logs/euler/compiler/gpu_default_run.log (fp64)
+# and logs/euler/fp32/run.log (fp32), "Execution Time" of the time loop.
+SHOCK_BUBBLE_A30_MS = {"fp64": 758.47, "fp32": 617.92}
+REF_EULER_GPU = os.path.join(ROOT, "oracle", "_ref", "euler2d_gpu_{}")
+
+
+def run_reference_euler_gpu(prec, reps=3, warmups=1):
+    """The reference's shock-bubble GPU program (src/euler/euler2d_cuda.cu,
+    recompiled unchanged for sm_100a into oracle/_ref/) on this GPU: its own
+    "Execution Time" line (host clock around the time loop), median of `reps`
+    runs after `warmups` untimed ones.  None where the binary is absent or a
+    run fails."""
+    exe = REF_EULER_GPU.format(prec)
+    if not os.path.exists(exe):
+        return None
+    env = dict(os.environ, OUTDIR="/dev/null/pmhd_no_output")
+    times, steps = [], None
+    for i in range(warmups + reps):
+        r = subprocess.run([exe], env=env, capture_output=True, text=True, timeout=300)
+        m = re.search(r"Execution Time: ([0-9.]+) ms", r.stdout)
+        k = re.search(r"Done\. Steps: (\d+)", r.stdout)
+        if r.returncode != 0 or not m or not k:
+            return None
+        if i >= warmups:
+            times.append(float(m.group(1)))
+            steps = int(k.group(1))
+    return {"ms": statistics.median(times), "steps": steps, "runs": reps, "warmup_runs": warmups}
+
+
+def bench_shock_bubble(pmhd, device, max_over_ranks, world, reference_gpu=True):
+    """The reference's shock-bubble program (Haas-Sturtevant, 500 x 197,
+    MUSCL-Hancock + HLLC, split x/y, to t = 0.0011741 s: 3459 steps) run
+    whole through the C ABI, fp64 and fp32, performance build: device time of
+    the time loop (CUDA events around it, host polling included) and host
+    wall time of pmhd_euler2d_advance, after one untimed whole run; against
+    the published A30 time of the reference's GPU program and, where built,
+    the same program on this GPU."""
+    out = {"grid": [500, 197], "problem": "shock-bubble (src/euler/euler2d_cpu.cpp), to t = 0.0011741 s"}
+    for prec in ("fp64", "fp32"):
+        with pmhd.Euler2D(config="shock_bubble", precision=prec, device=device) as e:
+            e.advance()
+        with pmhd.Euler2D(config="shock_bubble", precision=prec, device=device) as e:
+            t0 = time.perf_counter()
+            st = e.advance()
+            wall_ms = (time.perf_counter() - t0) * 1e3
+        ms = max_over_ranks(st.device_ms)
+        cells = 500 * 197 * st.steps
+        rec = {"steps": st.steps, "t": st.t, "device_ms": ms, "wall_ms": wall_ms,
+               "value": world * cells / (ms / 1e3), "unit": UNIT, "a30_published_ms": SHOCK_BUBBLE_A30_MS[prec],
+               "a30_published_value": cells / (SHOCK_BUBBLE_A30_MS[prec] / 1e3)}
+        ref = run_reference_euler_gpu(prec) if reference_gpu else None
+        if ref is not None:
+            rec["reference_gpu_same_box"] = ref
+        out[prec] = rec
+    return out
+
+
 def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, max_pairs=1500, seed=11,
                   kh=False, precision="mixed"):
     """Learned correction: training pairs from the solver (Orszag-Tang with
@@ -695,6 +753,8 @@ def main():
     euler = None
     if args.euler > 0:
         euler = bench_euler(pmhd, args.euler, W, K, local, max_over_ranks, world)
+        euler["shock_bubble"] = bench_shock_bubble(pmhd, local, max_over_ranks, world,
+                                                   reference_gpu=not args.no_compare and rank == 0)
 
     # ---- learned coarse-grid correction: accuracy and wall time ---------------
     learned = None

@@ -116,7 +116,7 @@ typedef struct {
   unsigned long long kernel_launches; /* kernels that did work, total        */
   double device_ms;                 /* GPU time of the last pmhd_advance, from
                                        CUDA events on the handle's stream     */
-  int tile_height;                  /* stage-kernel tile height in use (16, 8) */
+  int tile_height;                  /* stage-kernel tile height in use (19, 8) */
   int ctas;                         /* persistent CTAs per stage launch        */
   unsigned long long zone_cycles;   /* cells x steps of the last advance
                                        (summed over ensemble members)         */
@@ -397,8 +397,17 @@ typedef struct {
   int status;
 } pmhd_euler_stats;
 
+/* config of pmhd_euler2d_create for the shock-bubble program
+ * (src/euler/euler2d_cpu.cpp; Haas-Sturtevant: a Mach 1.22 shock in air
+ * meets a helium bubble, 0.225 x 0.089 m, reference grid 500 x 197, end time
+ * 0.0011741 s).  Its constants are binary64 literals
+ * (include/euler/config.hpp), so in binary32 the cell centres, the CFL
+ * product and the end-time tests are binary64 expressions, as there. */
+enum { PMHD_EULER_SHOCK_BUBBLE = 100 };
+
 /* nx x ny grid on [0,1]^2 holding Liska-Wendroff configuration `config`
- * (3, 6 or 12; riemann2d_cpu.cpp:54-76). */
+ * (3, 6 or 12; riemann2d_cpu.cpp:54-76), or the shock-bubble domain
+ * (config PMHD_EULER_SHOCK_BUBBLE). */
 int pmhd_euler2d_create(int nx, int ny, int config, int solver, int precision, int exact, int device,
                         pmhd_euler2d** out);
 /* Advances until t_end (< 0: the configuration's end time) or max_steps

@@ -4,8 +4,9 @@
  * euler_oracle.c.  TEST INFRASTRUCTURE ONLY: used by tests/ as the checker
  * of the GPU Euler kernels, never by the product.
  *
- * Follows src/euler/riemann1d_cpu.cpp:95-214 and
- * src/euler/riemann2d_cpu.cpp:108-330 (same loops, ghost handling and
+ * Follows src/euler/riemann1d_cpu.cpp:95-214,
+ * src/euler/riemann2d_cpu.cpp:108-330 and src/euler/euler2d_cpu.cpp:53-398
+ * (same loops, ghost handling and
  * expression order, gamma a binary64 constant as in
  * include/euler/config.hpp:43) with the point functions of
  * include/euler/euler_common.hpp and include/euler/riemann.hpp. */
@@ -186,24 +187,41 @@ static int EN(eo_lw_config)(int id, ET q[4][4], ET* t_end) {
   return 1;
 }
 
-/* 2D Riemann problem, NX x NY on [0,1]^2 (the reference runs N x N), CFL
- * 0.8, transmissive walls (riemann2d_cpu.cpp:108-330).  max_steps < 0: run
- * to T_end (t_end < 0: the configuration's).  out: primitive interior
- * [NY][NX][4] (rho, u, v, p).  Returns the step count, or -1 on a bad
- * configuration / allocation. */
-long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, long long max_steps, ET* out,
-                           ET* t_out) {
+/* Problem id of the shock-bubble program (src/euler/euler2d_cpu.cpp). */
+#ifndef EO_SHOCK_BUBBLE
+#define EO_SHOCK_BUBBLE 100
+#endif
+
+/* The 2D driver behind eo_riemann2d and eo_shock_bubble: NX x NY cells,
+ * CFL 0.8, transmissive walls, dimensionally split steps alternating x-y /
+ * y-x.  prob = 3, 6, 12 (riemann2d_cpu.cpp:108-330, [0,1]^2, every scalar
+ * of type ET) or EO_SHOCK_BUBBLE (euler2d_cpu.cpp:109-398: 0.225 x 0.089 m;
+ * include/euler/config.hpp gives the domain, CFL_NUM and T_END as binary64
+ * literals, so in the binary32 build the cell centres, the time step
+ * (CFL_NUM * min(...)) and every test against T_END are binary64
+ * expressions rounded to ET where they are stored). */
+static long long EN(eo_run2d)(int NX, int NY, int prob, int hll, double t_end_in, long long max_steps, ET* out,
+                              ET* t_out) {
   const int GH = 2, TX = NX + 4, TY = NY + 4;
   const size_t SZ = (size_t)TX * TY;
-  ET q[4][4], T_end;
+  const int sb = prob == EO_SHOCK_BUBBLE;
+  ET q[4][4], T_end = (ET)0;
+  double T_endd = 0.0;
   ET *rho, *ru, *rv, *E, *W[4], *WL[4], *WR[4], *WLh[4], *WRh[4], *F[4];
   ET* blk;
   int i, j, k, g;
   long long step = 0;
   ET t = (ET)0.0;
-  const ET dx = ((ET)1.0 - (ET)0.0) / (ET)NX, dy = ((ET)1.0 - (ET)0.0) / (ET)NY, cfl = (ET)0.8;
-  if (!EN(eo_lw_config)(cfg_id, q, &T_end) || NX < 2 || NY < 2) return -1;
-  if (t_end_in > (ET)0.0) T_end = t_end_in;
+  /* config.hpp:56-57: DX = (Real)(X_MAX - X_MIN) / (Real)NX; riemann2d: ((Real)1 - (Real)0) / N. */
+  const ET dx = sb ? (ET)(0.225 - 0.0) / (ET)NX : ((ET)1.0 - (ET)0.0) / (ET)NX;
+  const ET dy = sb ? (ET)(0.089 - 0.0) / (ET)NY : ((ET)1.0 - (ET)0.0) / (ET)NY, cfl = (ET)0.8;
+  if (NX < 2 || NY < 2) return -1;
+  if (sb) {
+    T_endd = t_end_in > 0.0 ? t_end_in : 0.0011741;
+  } else {
+    if (!EN(eo_lw_config)(prob, q, &T_end)) return -1;
+    if (t_end_in > 0.0) T_end = (ET)t_end_in;
+  }
   blk = (ET*)calloc(SZ * 24, sizeof(ET));
   if (!blk) return -1;
   rho = blk; ru = blk + SZ; rv = blk + 2 * SZ; E = blk + 3 * SZ;
@@ -213,17 +231,49 @@ long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, lon
     F[k] = WL[k]; /* the flux reuses the reconstruction buffers (not read after Hancock) */
   }
 #define ID(i_, j_) ((size_t)(j_) * TX + (i_))
-  for (j = 0; j < TY; j++) {
-    ET y = (ET)0.0 + (j - GH + (ET)0.5) * dy;
-    for (i = 0; i < TX; i++) {
-      ET x = (ET)0.0 + (i - GH + (ET)0.5) * dx;
-      const ET* s = (x >= (ET)0.5 && y >= (ET)0.5) ? q[0] : (x < (ET)0.5 && y >= (ET)0.5) ? q[1]
-                  : (x < (ET)0.5 && y < (ET)0.5) ? q[2] : q[3];
-      ET Wc[4] = {s[0], s[1], s[2], s[3]}, Uc[4];
-      size_t id = ID(i, j);
-      for (k = 0; k < 4; k++) W[k][id] = Wc[k];
-      EN(eo_p2c)(Wc, Uc);
-      rho[id] = Uc[0]; ru[id] = Uc[1]; rv[id] = Uc[2]; E[id] = Uc[3];
+  if (sb) {
+    /* euler2d_cpu.cpp:114-150: Rankine-Hugoniot post-shock state of a Mach
+     * 1.22 shock in air (ET arithmetic), a helium bubble of radius 2.5 cm at
+     * (3.5 cm, 4.45 cm), the shock at x = 0.5 cm. */
+    const ET M = (ET)1.22, gm = (ET)1.4, rho1 = (ET)1.29, p1 = (ET)101325.0;
+    const ET c1 = (ET)sqrt(gm * p1 / rho1);
+    const ET rho2 = rho1 * ((gm + 1) * M * M) / ((gm - 1) * M * M + 2);
+    const ET p2 = p1 * (2 * gm * M * M - (gm - 1)) / (gm + 1);
+    const ET u2 = c1 * M * (1 - rho1 / rho2);
+    const ET R2 = (ET)(0.025 * 0.025);
+    for (j = 0; j < TY; j++) {
+      const ET y = (ET)(0.0 + (j - GH + 0.5) * (double)dy);
+      for (i = 0; i < TX; i++) {
+        const ET x = (ET)(0.0 + (i - GH + 0.5) * (double)dx);
+        const ET dxb = (ET)((double)x - 0.035), dyb = (ET)((double)y - 0.089 / 2.0);
+        const ET d2 = dxb * dxb + dyb * dyb;
+        ET Wc[4], Uc[4];
+        size_t id = ID(i, j);
+        if (d2 < R2) {
+          Wc[0] = (ET)0.214; Wc[1] = (ET)0.0; Wc[2] = (ET)0.0; Wc[3] = p1;
+        } else if ((double)x < 0.005) {
+          Wc[0] = rho2; Wc[1] = u2; Wc[2] = (ET)0.0; Wc[3] = p2;
+        } else {
+          Wc[0] = rho1; Wc[1] = (ET)0.0; Wc[2] = (ET)0.0; Wc[3] = p1;
+        }
+        for (k = 0; k < 4; k++) W[k][id] = Wc[k];
+        EN(eo_p2c)(Wc, Uc);
+        rho[id] = Uc[0]; ru[id] = Uc[1]; rv[id] = Uc[2]; E[id] = Uc[3];
+      }
+    }
+  } else {
+    for (j = 0; j < TY; j++) {
+      ET y = (ET)0.0 + (j - GH + (ET)0.5) * dy;
+      for (i = 0; i < TX; i++) {
+        ET x = (ET)0.0 + (i - GH + (ET)0.5) * dx;
+        const ET* s = (x >= (ET)0.5 && y >= (ET)0.5) ? q[0] : (x < (ET)0.5 && y >= (ET)0.5) ? q[1]
+                    : (x < (ET)0.5 && y < (ET)0.5) ? q[2] : q[3];
+        ET Wc[4] = {s[0], s[1], s[2], s[3]}, Uc[4];
+        size_t id = ID(i, j);
+        for (k = 0; k < 4; k++) W[k][id] = Wc[k];
+        EN(eo_p2c)(Wc, Uc);
+        rho[id] = Uc[0]; ru[id] = Uc[1]; rv[id] = Uc[2]; E[id] = Uc[3];
+      }
     }
   }
 #define BC()                                                                                   \
@@ -250,7 +300,7 @@ long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, lon
     }                                                                 \
   } while (0)
   BC();
-  while (t < T_end && (max_steps < 0 || step < max_steps)) {
+  while ((sb ? (double)t < T_endd : t < T_end) && (max_steps < 0 || step < max_steps)) {
     ET mx = (ET)0, my = (ET)0, dt;
     int pass;
     C2P();
@@ -261,8 +311,14 @@ long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, lon
         mx = EN(eo_max)(mx, (ET)fabs(W[1][id]) + c);
         my = EN(eo_max)(my, (ET)fabs(W[2][id]) + c);
       }
-    dt = cfl * EN(eo_min)(dx / mx, dy / my);
-    if (t + dt > T_end) dt = T_end - t;
+    if (sb) {
+      /* euler2d_cpu.cpp:165 and :306-309 */
+      dt = (ET)(0.8 * (double)EN(eo_min)(dx / mx, dy / my));
+      if ((double)(ET)(t + dt) > T_endd) dt = (ET)(T_endd - (double)t);
+    } else {
+      dt = cfl * EN(eo_min)(dx / mx, dy / my);
+      if (t + dt > T_end) dt = T_end - t;
+    }
     if (dt <= (ET)0.0 || t + dt == t) break;
     for (pass = 0; pass < 2; pass++) {
       const int xsweep = ((step % 2 == 0) ? pass == 0 : pass == 1);
@@ -347,6 +403,25 @@ long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, lon
 #undef ID
   free(blk);
   return step;
+}
+
+/* 2D Riemann problem, NX x NY on [0,1]^2 (the reference runs N x N), CFL
+ * 0.8, transmissive walls (riemann2d_cpu.cpp:108-330).  max_steps < 0: run
+ * to T_end (t_end < 0: the configuration's).  out: primitive interior
+ * [NY][NX][4] (rho, u, v, p).  Returns the step count, or -1 on a bad
+ * configuration / allocation. */
+long long EN(eo_riemann2d)(int NX, int NY, int cfg_id, int hll, ET t_end_in, long long max_steps, ET* out,
+                           ET* t_out) {
+  if (cfg_id == EO_SHOCK_BUBBLE) return -1;
+  return EN(eo_run2d)(NX, NY, cfg_id, hll, (double)t_end_in, max_steps, out, t_out);
+}
+
+/* Shock-bubble problem (euler2d_cpu.cpp, Haas-Sturtevant: Mach 1.22 shock in
+ * air on a helium bubble; the reference grid is 500 x 197) on NX x NY cells of
+ * the 0.225 x 0.089 m domain, to T_END = 0.0011741 s (t_end <= 0) or t_end.
+ * Arguments and result as eo_riemann2d. */
+long long EN(eo_shock_bubble)(int NX, int NY, int hll, double t_end_in, long long max_steps, ET* out, ET* t_out) {
+  return EN(eo_run2d)(NX, NY, EO_SHOCK_BUBBLE, hll, t_end_in, max_steps, out, t_out);
 }
 
 /* Toro test states (riemann1d_cpu.cpp:43-62): rhoL uL pL rhoR uR pR T_end x0. */

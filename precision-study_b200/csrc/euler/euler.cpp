@@ -1,7 +1,7 @@
 // euler.cpp -- pmhd_euler2d_* / pmhd_euler1d_run (include/pmhd.h): host side
 // of the Euler sibling.  Initial states follow the reference programs
-// (src/euler/riemann2d_cpu.cpp:117-134, src/euler/riemann1d_cpu.cpp:95-112)
-// with the same arithmetic; the 2D time loop replays CUDA graphs of
+// (src/euler/riemann2d_cpu.cpp:117-134, src/euler/euler2d_cpu.cpp:109-150,
+// src/euler/riemann1d_cpu.cpp:95-112) with the same arithmetic; the 2D time loop replays CUDA graphs of
 // fused split steps (state ping-ponged between two SoA buffers) and polls
 // the device control block one replay behind.
 #include <cuda_runtime.h>
@@ -20,7 +20,7 @@
 using namespace pmhd::euler;
 
 struct pmhd_euler2d {
-  int nx = 0, ny = 0, pitch = 0, config = 0, hll = 0, fp32 = 0, exact = 0, device = 0;
+  int nx = 0, ny = 0, pitch = 0, config = 0, hll = 0, fp32 = 0, exact = 0, device = 0, wide_time = 0;
   long long plane = 0;
   size_t elem = 8;
   double dx = 0, dy = 0, cfl = 0, t_end_cfg = 0;
@@ -102,6 +102,43 @@ void init_2d(const pmhd_euler2d* e, const double qd[4][4], std::vector<unsigned 
                  : (x < (T)0.5 && y < (T)0.5) ? q[2] : q[3];
       T U[4];
       prim_to_cons(s, U);
+      for (int k = 0; k < 4; k++) u[(size_t)k * e->plane + (size_t)j * e->pitch + i] = U[k];
+    }
+  }
+}
+
+// Shock-bubble initial state (euler2d_cpu.cpp:109-150): the post-shock state
+// of a Mach 1.22 shock in air from the Rankine-Hugoniot relations (T
+// arithmetic), a helium bubble of radius 2.5 cm centred at (3.5, 4.45) cm,
+// the shock at x = 0.5 cm.  Cell centres and the comparisons with the
+// binary64 constants are binary64 expressions, as in the reference.
+template <class T>
+void init_shock_bubble(const pmhd_euler2d* e, std::vector<unsigned char>& buf) {
+  buf.assign((size_t)4 * e->plane * sizeof(T), 0);
+  T* u = reinterpret_cast<T*>(buf.data());
+  const T M = (T)1.22, g = (T)1.4, rho1 = (T)1.29, p1 = (T)101325.0;
+  const T c1 = std::sqrt(g * p1 / rho1);
+  const T rho2 = rho1 * ((g + 1) * M * M) / ((g - 1) * M * M + 2);
+  const T p2 = p1 * (2 * g * M * M - (g - 1)) / (g + 1);
+  const T u2 = c1 * M * (1 - rho1 / rho2);
+  const T R2 = (T)(0.025 * 0.025);
+  const double dx = (double)e->dx, dy = (double)e->dy;
+  for (int j = 0; j < e->ny; j++) {
+    const T y = (T)(0.0 + (j + 0.5) * dy);
+    for (int i = 0; i < e->nx; i++) {
+      const T x = (T)(0.0 + (i + 0.5) * dx);
+      const T dxb = (T)((double)x - 0.035), dyb = (T)((double)y - 0.089 / 2.0);
+      const T d2 = dxb * dxb + dyb * dyb;
+      T W[4];
+      if (d2 < R2) {
+        W[0] = (T)0.214, W[1] = (T)0.0, W[2] = (T)0.0, W[3] = p1;
+      } else if ((double)x < 0.005) {
+        W[0] = rho2, W[1] = u2, W[2] = (T)0.0, W[3] = p2;
+      } else {
+        W[0] = rho1, W[1] = (T)0.0, W[2] = (T)0.0, W[3] = p1;
+      }
+      T U[4];
+      prim_to_cons(W, U);
       for (int k = 0; k < 4; k++) u[(size_t)k * e->plane + (size_t)j * e->pitch + i] = U[k];
     }
   }
@@ -228,8 +265,10 @@ int pmhd_euler2d_create(int nx, int ny, int config, int solver, int precision, i
                         pmhd_euler2d** out) {
   if (!out) return PMHD_ERR_ARG;
   *out = nullptr;
-  double q[4][4], t_end;
-  if (nx < 2 || ny < 2 || (long long)nx * ny > (1LL << 31) || !lw_config(config, q, &t_end)) return PMHD_ERR_ARG;
+  double q[4][4], t_end = 0.0011741;  // euler2d: T_END (include/euler/config.hpp)
+  const bool sb = config == PMHD_EULER_SHOCK_BUBBLE;
+  if (nx < 2 || ny < 2 || (long long)nx * ny > (1LL << 31) || (!sb && !lw_config(config, q, &t_end)))
+    return PMHD_ERR_ARG;
   if (solver != PMHD_SOLVER_HLL && solver != PMHD_SOLVER_HLLC) return PMHD_ERR_ARG;
   if (precision != PMHD_FP64 && precision != PMHD_FP32) return PMHD_ERR_ARG;
   int rc = check_device(device);
@@ -249,18 +288,28 @@ int pmhd_euler2d_create(int nx, int ny, int config, int solver, int precision, i
   e->device = device;
   e->elem = e->fp32 ? 4 : 8;
   e->t_end_cfg = t_end;
+  e->wide_time = sb ? 1 : 0;
+  // Domain lengths: [0,1]^2, or the shock-bubble's X_MAX - X_MIN and Y_MAX - Y_MIN
+  // (binary64 differences, rounded to the run's type as config.hpp's DX / DY do).
+  const double lx = sb ? 0.225 - 0.0 : 1.0, ly = sb ? 0.089 - 0.0 : 1.0;
   std::vector<unsigned char> host;
   if (e->fp32) {
-    const float dx = (1.0f - 0.0f) / (float)nx, dy = (1.0f - 0.0f) / (float)ny;
+    const float dx = (float)lx / (float)nx, dy = (float)ly / (float)ny;
     e->dx = dx;
     e->dy = dy;
-    e->cfl = (double)0.8f;
-    init_2d<float>(e, q, host);
+    e->cfl = sb ? 0.8 : (double)0.8f;
+    if (sb)
+      init_shock_bubble<float>(e, host);
+    else
+      init_2d<float>(e, q, host);
   } else {
-    e->dx = (1.0 - 0.0) / nx;
-    e->dy = (1.0 - 0.0) / ny;
+    e->dx = lx / nx;
+    e->dy = ly / ny;
     e->cfl = 0.8;
-    init_2d<double>(e, q, host);
+    if (sb)
+      init_shock_bubble<double>(e, host);
+    else
+      init_2d<double>(e, q, host);
   }
   const size_t bytes = (size_t)4 * e->plane * e->elem;
   bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -287,7 +336,7 @@ int pmhd_euler2d_advance(pmhd_euler2d* e, double t_end, long long max_steps, pmh
   if (!e) return PMHD_ERR_ARG;
   E_CU(cudaSetDevice(e->device));
   if (t_end < 0) t_end = e->t_end_cfg;
-  if (e->fp32) t_end = (double)(float)t_end;
+  if (e->fp32 && !e->wide_time) t_end = (double)(float)t_end;
   EulerCtrl& h = e->hctrl[0];
   std::memset(&h, 0, sizeof(h));
   h.t[0] = h.t[1] = e->t;
@@ -295,6 +344,8 @@ int pmhd_euler2d_advance(pmhd_euler2d* e, double t_end, long long max_steps, pmh
   h.t_end = t_end;
   h.step_limit = max_steps < 0 ? LLONG_MAX : e->steps + max_steps;
   h.stop = e->stopped ? 1 : 0;
+  h.wide_time = e->wide_time;
+  h.cfl = e->cfl;
   E_CU(cudaMemcpyAsync(e->dctrl, &h, sizeof(h), cudaMemcpyHostToDevice, e->stream));
   E_CU(cudaEventRecord(e->ev0, e->stream));
   const int slot = (int)(e->steps % 3);

@@ -15,10 +15,11 @@ struct EulerCtrl {
   double t[2];
   long long step[2];
   unsigned long long sx[3], sy[3];
-  double t_end;
+  double t_end;  // compared with t in binary64 (t_end holds a value of the run's type unless wide_time)
   long long step_limit;
-  int stop;  // the reference's "dt <= 0 or t + dt == t" exit was taken
-  int pad;
+  int stop;       // the reference's "dt <= 0 or t + dt == t" exit was taken
+  int wide_time;  // binary64 CFL and end-time arithmetic of the shock-bubble program (euler2d_cpu.cpp:165, :306)
+  double cfl;     // the CFL number as binary64 (used when wide_time)
 };
 
 #define PMHD_EULER_DECLARE(NS)                                                                                      \

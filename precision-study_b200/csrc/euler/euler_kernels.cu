@@ -132,21 +132,23 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
   // other parity and the speed slot two steps ahead).
   const T t = (T)ctrl->t[p];
   const long long n = ctrl->step[p];
-  bool active = !ctrl->stop && t < (T)ctrl->t_end && n < ctrl->step_limit;
+  // t and t + dt are values of type T, so their tests against t_end are
+  // exact in binary64 whichever type t_end has.
+  bool active = !ctrl->stop && (double)t < ctrl->t_end && n < ctrl->step_limit;
   T dt = (T)0;
   if (active) {
     const T mx = (T)bits_speed(ctrl->sx[n % 3]), my = (T)bits_speed(ctrl->sy[n % 3]);
-    dt = cfl * vmin(dx / mx, dy / my);
-    const T t_end = (T)ctrl->t_end;
-    if (t + dt > t_end) dt = t_end - t;
-    if (!(dt > (T)0.0) || t + dt == t) active = false;  // riemann2d_cpu.cpp:298
+    const T m = vmin(dx / mx, dy / my);
+    dt = ctrl->wide_time ? (T)(ctrl->cfl * (double)m) : cfl * m;
+    if ((double)(T)(t + dt) > ctrl->t_end) dt = ctrl->wide_time ? (T)(ctrl->t_end - (double)t) : (T)ctrl->t_end - t;
+    if (!(dt > (T)0.0) || t + dt == t) active = false;  // riemann2d_cpu.cpp:298, euler2d_cpu.cpp:309
   }
   const bool leader = blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0;
   if (!active) {
     if (leader) {
       ctrl->t[p ^ 1] = ctrl->t[p];
       ctrl->step[p ^ 1] = n;
-      if (!(t < (T)ctrl->t_end) || n >= ctrl->step_limit) {
+      if (!((double)t < ctrl->t_end) || n >= ctrl->step_limit) {
       } else {
         ctrl->stop = 1;
       }

@@ -521,14 +521,27 @@ def _euler_solver(solver):
     return SOLVER_HLL if solver == "hll" else SOLVER_HLLC
 
 
-class Euler2D:
-    """The Euler sibling's 2D Riemann problem (a pmhd_euler2d handle):
-    Liska-Wendroff configuration 3, 6 or 12 on an nx x ny grid."""
+EULER_SHOCK_BUBBLE = 100  # PMHD_EULER_SHOCK_BUBBLE
 
-    def __init__(self, nx, ny=None, config=3, solver="hllc", precision="fp64", exact=False, device=0):
+
+class Euler2D:
+    """The Euler sibling's 2D problems (a pmhd_euler2d handle): Liska-Wendroff
+    configuration 3, 6 or 12 on an nx x ny grid of [0,1]^2
+    (src/euler/riemann2d_cpu.cpp), or config="shock_bubble" (EULER_SHOCK_BUBBLE):
+    the Haas-Sturtevant shock-bubble program (src/euler/euler2d_cpu.cpp) on
+    nx x ny cells of its 0.225 x 0.089 m domain (the reference's grid is
+    500 x 197, the default here)."""
+
+    def __init__(self, nx=None, ny=None, config=3, solver="hllc", precision="fp64", exact=False, device=0):
+        if config == "shock_bubble":
+            config = EULER_SHOCK_BUBBLE
+        if config == EULER_SHOCK_BUBBLE:
+            nx = 500 if nx is None else nx
+            ny = 197 if ny is None else ny
         ny = nx if ny is None else ny
-        self.nx, self.ny = nx, ny
+        self.nx, self.ny, self.config, self.precision = nx, ny, config, precision
         self.dtype = np.float32 if precision == "fp32" else np.float64
+        self.steps, self.t = 0, 0.0
         h = ctypes.c_void_p()
         _check(load().pmhd_euler2d_create(nx, ny, config, _euler_solver(solver), PRECISIONS[precision],
                                           int(bool(exact)), device, ctypes.byref(h)), "pmhd_euler2d_create")
@@ -554,12 +567,38 @@ class Euler2D:
     def advance(self, t_end=-1.0, max_steps=-1):
         st = EulerStats()
         _check(load().pmhd_euler2d_advance(self._h, t_end, max_steps, ctypes.byref(st)), "pmhd_euler2d_advance")
+        self.steps, self.t = st.steps, st.t
         return st
 
     def prims(self):
         out = np.empty((self.ny, self.nx, 4), dtype=self.dtype)
         _check(load().pmhd_euler2d_get_prim(self._h, out.ctypes.data), "pmhd_euler2d_get_prim")
         return out
+
+    def write_dat(self, path):
+        """Writes the state as the shock-bubble program's .dat file
+        (src/euler/euler2d_cpu.cpp:375-395): three '#' header lines (time,
+        steps, end time), then x outermost, one 'x y rho u v p' line per cell in
+        scientific notation with max_digits10 digits, a blank line after each
+        column; cell centres are binary64 expressions stored in the
+        precision's type, as there.  Returns path."""
+        if self.config != EULER_SHOCK_BUBBLE:
+            raise PmhdError(ERR_ARG, "write_dat (the .dat layout is the shock-bubble program's)")
+        T = self.dtype
+        f = "%.9e" if T == np.float32 else "%.17e"
+        dx = float(T(T(0.225 - 0.0) / T(self.nx)))
+        dy = float(T(T(0.089 - 0.0) / T(self.ny)))
+        w = self.prims()
+        ys = [f % float(T(0.0 + (j + 0.5) * dy)) for j in range(self.ny)]
+        with open(path, "w") as out:
+            out.write("# Time = %s\n# Steps = %d\n# T_END = %s\n" % (f % float(T(self.t)), self.steps, f % 0.0011741))
+            for i in range(self.nx):
+                x = f % float(T(0.0 + (i + 0.5) * dx))
+                col = w[:, i, :]
+                out.write("".join(x + " " + ys[j] + " " + " ".join(f % float(v) for v in col[j]) + "\n"
+                                  for j in range(self.ny)))
+                out.write("\n")
+        return path
 
 
 def euler1d(n, test, solver="hllc", precision="fp64", exact=False, device=0):

@@ -37,6 +37,21 @@ def riemann2d(n, config, solver="hllc", prec="fp64", t_end=-1.0, max_steps=-1, n
     return steps, t.value, out
 
 
+def shock_bubble(nx=500, ny=197, solver="hllc", prec="fp64", t_end=-1.0, max_steps=-1):
+    """Oracle shock-bubble run (src/euler/euler2d_cpu.cpp) on nx x ny:
+    (steps, t, prims [ny][nx][4])."""
+    T = _ctype(prec)
+    fn = getattr(_lib(), "eo_shock_bubble_" + ("f64" if prec == "fp64" else "f32"))
+    fn.restype = ctypes.c_longlong
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p,
+                   ctypes.POINTER(T)]
+    out = np.zeros((ny, nx, 4), dtype=_np(prec))
+    t = T()
+    steps = fn(nx, ny, 1 if solver == "hll" else 0, t_end, max_steps, out.ctypes.data, ctypes.byref(t))
+    assert steps >= 0
+    return steps, t.value, out
+
+
 def riemann1d(n, test, solver="hllc", prec="fp64"):
     """Oracle 1D Riemann run: (steps, t, [n][3] = rho, u, p)."""
     T = _ctype(prec)
@@ -67,6 +82,27 @@ def dat_md5_2d(prims, prec):
             x = T(0.0) + (T(i) + T(0.5)) * dx
             vals = (x, y) + tuple(prims[j, i])
             lines.append(" ".join(f % float(v) for v in vals) + "\n")
+    return hashlib.md5("".join(lines).encode()).hexdigest()
+
+
+def dat_md5_shock_bubble(prims, prec):
+    """md5 of the data lines (those not starting with '#') of the .dat file
+    src/euler/euler2d_cpu.cpp:378-394 writes: x outermost, one line per cell
+    (x y rho u v p), a blank line after each column; cell centres are
+    binary64 expressions (config.hpp literals) stored in the precision's
+    type."""
+    ny, nx = prims.shape[:2]
+    T = _np(prec)
+    dx = float(T(T(0.225 - 0.0) / T(nx)))
+    dy = float(T(T(0.089 - 0.0) / T(ny)))
+    f = _fmt(prec)
+    ys = [f % float(T(0.0 + (j + 0.5) * dy)) for j in range(ny)]
+    lines = []
+    for i in range(nx):
+        x = f % float(T(0.0 + (i + 0.5) * dx))
+        for j in range(ny):
+            lines.append(x + " " + ys[j] + " " + " ".join(f % float(v) for v in prims[j, i]) + "\n")
+        lines.append("\n")
     return hashlib.md5("".join(lines).encode()).hexdigest()
 
 

@@ -51,3 +51,21 @@ def test_exact_solver_conserves_the_sod_star_state():
     # Toro (2009) table 4.2, test 1: p* = 0.30313, u* = 0.92745.
     p, u = exact_riemann.star_state(1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
     assert abs(p - 0.30313) < 5e-6 and abs(u - 0.92745) < 5e-6
+
+
+def test_oracle_shock_bubble_reproduces_the_reference_output(oracle):
+    """The shock-bubble program (src/euler/euler2d_cpu.cpp) at its own grid,
+    500 x 197 to t = 0.0011741 s (3459 steps): step count, final time and the
+    md5 of the .dat data lines equal the reference program's, binary64 and
+    binary32 (whose time control mixes in binary64 constants).  The two runs
+    go concurrently (ctypes releases the GIL during the oracle call)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    runs = GOLD["shock_bubble"]
+    with ThreadPoolExecutor(len(runs)) as ex:
+        results = list(ex.map(lambda r: EL.shock_bubble(r["nx"], r["ny"], r["solver"], r["precision"]), runs))
+    for run, (steps, t, prims) in zip(runs, results):
+        T = np.float64 if run["precision"] == "fp64" else np.float32
+        assert steps == run["steps"], run["precision"]
+        assert T(t) == T(run["t"]), run["precision"]
+        assert EL.dat_md5_shock_bubble(prims, run["precision"]) == run["md5_data"], run["precision"]
