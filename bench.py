@@ -632,6 +632,7 @@ def main():
     ap.add_argument("--learned", type=int, default=512, help="coarse grid of the learned-correction line (0: skip)")
     ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
     ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
+    ap.add_argument("--shock-bubble", type=int, default=1, help="whole shock-bubble runs in the Euler line (0: skip)")
     ap.add_argument("--hancock", type=int, default=4096, help="grid of the MUSCL-Hancock line (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -753,8 +754,9 @@ def main():
     euler = None
     if args.euler > 0:
         euler = bench_euler(pmhd, args.euler, W, K, local, max_over_ranks, world)
-        euler["shock_bubble"] = bench_shock_bubble(pmhd, local, max_over_ranks, world,
-                                                   reference_gpu=not args.no_compare and rank == 0)
+        if args.shock_bubble:
+            euler["shock_bubble"] = bench_shock_bubble(pmhd, local, max_over_ranks, world,
+                                                       reference_gpu=not args.no_compare and rank == 0)
 
     # ---- learned coarse-grid correction: accuracy and wall time ---------------
     learned = None

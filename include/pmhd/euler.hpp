@@ -297,6 +297,154 @@ __host__ __device__ inline void hll_flux_1d(const T WL[3], const T WR[3], T f[3]
   }
 }
 
+// ---- performance forms (the fast build's 2D kernels) -------------------------
+// The same scheme with cheaper arithmetic, not bit-identical to the reference:
+//   * every expression in the run's type T (the reference evaluates the gamma
+//     expressions of its binary32 build in binary64);
+//   * one reciprocal per density or divisor, shared by its quotients, and
+//     1 / (gamma - 1) as the constant 2.5 (binary64: the IEEE reciprocal;
+//     binary32: the hardware's approximate reciprocal and square root);
+//   * the two Hancock faces of a cell share one flux difference (it depends
+//     only on the two face states, riemann.hpp:60-88 forms it twice);
+//   * the HLLC star energy as coeff (E/rho + (S* - u) S*) + (S* - u) p / (S - S*),
+//     the reference's coeff (E/rho + (S* - u)(S* + p / (rho (S - u)))) with
+//     coeff = rho (S - u) / (S - S*) distributed.
+#if defined(__CUDACC__)
+namespace fastform {
+
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ double root(double x) { return sqrt(x); }
+__device__ __forceinline__ float root(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <class T>
+__device__ __forceinline__ void cons_to_prim(const T U[4], T W[4]) {
+  const T ri = rcp(U[0]);
+  W[0] = U[0];
+  W[1] = U[1] * ri;
+  W[2] = U[2] * ri;
+  W[3] = (T)0.4 * (U[3] - (T)0.5 * (U[1] * W[1] + U[2] * W[2]));
+}
+
+// |u| + c and |v| + c of a conservative cell (the time-step reduction).
+template <class T>
+__device__ __forceinline__ void cell_speeds(const T U[4], T& sx, T& sy) {
+  const T ri = rcp(U[0]);
+  const T u = U[1] * ri, v = U[2] * ri;
+  const T p = (T)0.4 * (U[3] - (T)0.5 * (U[1] * u + U[2] * v));
+  const T c = root((T)1.4 * p * ri);
+  sx = std::fabs(u) + c;
+  sy = std::fabs(v) + c;
+}
+
+// Both Hancock-evolved faces of a cell from its reconstructed left / right
+// (lower / upper) face primitives.
+template <class T, int NI, int TI>
+__device__ __forceinline__ void hancock_pair(const T Wl[4], const T Wr[4], T Lh[4], T Rh[4], T fac) {
+  const T rL = Wl[0], uL = Wl[NI], vL = Wl[TI], pL = Wl[3];
+  const T rR = Wr[0], uR = Wr[NI], vR = Wr[TI], pR = Wr[3];
+  const T mL = rL * uL, mR = rR * uR;
+  const T EL = pL * (T)2.5 + (T)0.5 * rL * (uL * uL + vL * vL);
+  const T ER = pR * (T)2.5 + (T)0.5 * rR * (uR * uR + vR * vR);
+  T dF[4], UL[4], UR[4];
+  dF[0] = mR - mL;
+  dF[NI] = (mR * uR + pR) - (mL * uL + pL);
+  dF[TI] = mR * vR - mL * vL;
+  dF[3] = (ER + pR) * uR - (EL + pL) * uL;
+  UL[0] = rL, UL[NI] = mL, UL[TI] = rL * vL, UL[3] = EL;
+  UR[0] = rR, UR[NI] = mR, UR[TI] = rR * vR, UR[3] = ER;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    UL[k] -= fac * dF[k];
+    UR[k] -= fac * dF[k];
+  }
+  cons_to_prim(UL, Lh);
+  cons_to_prim(UR, Rh);
+}
+
+template <class T, int NI, int TI>
+__device__ __forceinline__ void hllc_flux(const T WL[4], const T WR[4], T f[4]) {
+  const T rhoL = WL[0], uL = WL[NI], vL = WL[TI], pL = WL[3];
+  const T rhoR = WR[0], uR = WR[NI], vR = WR[TI], pR = WR[3];
+  const T riL = rcp(rhoL), riR = rcp(rhoR);
+  const T cL = root((T)1.4 * pL * riL), cR = root((T)1.4 * pR * riR);
+  const T SL = vmin(uL - cL, uR - cR);
+  const T SR = vmax(uL + cL, uR + cR);
+  const T aL = rhoL * (SL - uL), aR = rhoR * (SR - uR);
+  const T Ss = (pR - pL + aL * uL - aR * uR) * rcp(aL - aR);
+  const T mL = rhoL * uL, mR = rhoR * uR;
+  const T EL = pL * (T)2.5 + (T)0.5 * rhoL * (uL * uL + vL * vL);
+  const T ER = pR * (T)2.5 + (T)0.5 * rhoR * (uR * uR + vR * vR);
+  if (SL > (T)0.0) {
+    f[0] = mL;
+    f[NI] = mL * uL + pL;
+    f[TI] = mL * vL;
+    f[3] = (EL + pL) * uL;
+  } else if (Ss > (T)0.0) {
+    const T d = rcp(SL - Ss), coeff = aL * d, su = Ss - uL;
+    const T U3 = coeff * (EL * riL + su * Ss) + su * pL * d;
+    f[0] = mL + SL * (coeff - rhoL);
+    f[NI] = (mL * uL + pL) + SL * (coeff * Ss - mL);
+    f[TI] = mL * vL + SL * (coeff * vL - rhoL * vL);
+    f[3] = (EL + pL) * uL + SL * (U3 - EL);
+  } else if (SR > (T)0.0) {
+    const T d = rcp(SR - Ss), coeff = aR * d, su = Ss - uR;
+    const T U3 = coeff * (ER * riR + su * Ss) + su * pR * d;
+    f[0] = mR + SR * (coeff - rhoR);
+    f[NI] = (mR * uR + pR) + SR * (coeff * Ss - mR);
+    f[TI] = mR * vR + SR * (coeff * vR - rhoR * vR);
+    f[3] = (ER + pR) * uR + SR * (U3 - ER);
+  } else {
+    f[0] = mR;
+    f[NI] = mR * uR + pR;
+    f[TI] = mR * vR;
+    f[3] = (ER + pR) * uR;
+  }
+}
+
+template <class T, int NI, int TI>
+__device__ __forceinline__ void hll_flux(const T WL[4], const T WR[4], T f[4]) {
+  const T rhoL = WL[0], uL = WL[NI], vL = WL[TI], pL = WL[3];
+  const T rhoR = WR[0], uR = WR[NI], vR = WR[TI], pR = WR[3];
+  const T cL = root((T)1.4 * pL * rcp(rhoL)), cR = root((T)1.4 * pR * rcp(rhoR));
+  const T SL = vmin(uL - cL, uR - cR);
+  const T SR = vmax(uL + cL, uR + cR);
+  const T mL = rhoL * uL, mR = rhoR * uR;
+  const T EL = pL * (T)2.5 + (T)0.5 * rhoL * (uL * uL + vL * vL);
+  const T ER = pR * (T)2.5 + (T)0.5 * rhoR * (uR * uR + vR * vR);
+  T FL[4], FR[4], UL[4], UR[4];
+  FL[0] = mL, FR[0] = mR;
+  FL[NI] = mL * uL + pL, FR[NI] = mR * uR + pR;
+  FL[TI] = mL * vL, FR[TI] = mR * vR;
+  FL[3] = (EL + pL) * uL, FR[3] = (ER + pR) * uR;
+  UL[0] = rhoL, UR[0] = rhoR;
+  UL[NI] = mL, UR[NI] = mR;
+  UL[TI] = rhoL * vL, UR[TI] = rhoR * vR;
+  UL[3] = EL, UR[3] = ER;
+  if (SL > (T)0.0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) f[k] = FL[k];
+  } else if (SR > (T)0.0) {
+    const T inv = rcp(SR - SL);
+#pragma unroll
+    for (int k = 0; k < 4; k++) f[k] = (SR * FL[k] - SL * FR[k] + SL * SR * (UR[k] - UL[k])) * inv;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) f[k] = FR[k];
+  }
+}
+
+}  // namespace fastform
+#endif
+
 }  // namespace euler
 }  // namespace pmhd
 

@@ -36,7 +36,59 @@ namespace PMHD_EKNS {
 
 namespace {
 
+// Point arithmetic of the build: the reference's expressions (exact build,
+// bit parity) or the performance forms (fast build, PMHD_EULER_FAST).
+#if PMHD_EULER_FAST
+namespace pf = ::pmhd::euler::fastform;
+template <class T>
+__device__ __forceinline__ void k_c2p(const T U[4], T W[4]) {
+  pf::cons_to_prim(U, W);
+}
+template <class T, int NI, int TI>
+__device__ __forceinline__ void k_hancock_pair(const T l[4], const T r[4], T lh[4], T rh[4], T fac) {
+  pf::hancock_pair<T, NI, TI>(l, r, lh, rh, fac);
+}
+template <class T, int NI, int TI, bool HLL>
+__device__ __forceinline__ void k_flux(const T a[4], const T b[4], T f[4]) {
+  if (HLL)
+    pf::hll_flux<T, NI, TI>(a, b, f);
+  else
+    pf::hllc_flux<T, NI, TI>(a, b, f);
+}
+template <class T>
+__device__ __forceinline__ void k_speeds(const T U[4], T& sx, T& sy) {
+  pf::cell_speeds(U, sx, sy);
+}
+#else
+template <class T>
+__device__ __forceinline__ void k_c2p(const T U[4], T W[4]) {
+  cons_to_prim(U, W);
+}
+template <class T, int NI, int TI>
+__device__ __forceinline__ void k_hancock_pair(const T l[4], const T r[4], T lh[4], T rh[4], T fac) {
+  hancock<T, NI, TI>(l, l, r, lh, fac);
+  hancock<T, NI, TI>(r, l, r, rh, fac);
+}
+template <class T, int NI, int TI, bool HLL>
+__device__ __forceinline__ void k_flux(const T a[4], const T b[4], T f[4]) {
+  if (HLL)
+    hll_flux<T, NI, TI>(a, b, f);
+  else
+    hllc_flux<T, NI, TI>(a, b, f);
+}
+// riemann2d_cpu.cpp:200-210: |u| + c, |v| + c from the primitives.
+template <class T>
+__device__ __forceinline__ void k_speeds(const T U[4], T& sx, T& sy) {
+  T W[4];
+  cons_to_prim(U, W);
+  const T cs = sound_speed(W[3], W[0]);
+  sx = std::fabs(W[1]) + cs;
+  sy = std::fabs(W[2]) + cs;
+}
+#endif
+
 constexpr int NV = 4;
+
 constexpr int TW = 32;  // tile width (cells)
 constexpr int RW = TW + 4;
 
@@ -80,8 +132,7 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
     T l[NV], r[NV], lh[NV], rh[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) muscl_recon(s.W[k][id - step], s.W[k][id], s.W[k][id + step], l[k], r[k]);
-    hancock<T, NI, TI>(l, l, r, lh, fac);
-    hancock<T, NI, TI>(r, l, r, rh, fac);
+    k_hancock_pair<T, NI, TI>(l, r, lh, rh, fac);
 #pragma unroll
     for (int k = 0; k < NV; k++) {
       s.HL[k][id] = lh[k];
@@ -101,10 +152,7 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
       a[k] = s.HR[k][id - step];
       b[k] = s.HL[k][id];
     }
-    if (HLL)
-      hll_flux<T, NI, TI>(a, b, f);
-    else
-      hllc_flux<T, NI, TI>(a, b, f);
+    k_flux<T, NI, TI, HLL>(a, b, f);
 #pragma unroll
     for (int k = 0; k < NV; k++) s.W[k][id] = f[k];
   }
@@ -169,7 +217,9 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
     ctrl->sy[(n + 2) % 3] = 0ull;
   }
   // Region load with wall clamping, and the primitives of every region cell
-  // (same thread, so no barrier between them).
+  // (same thread, so no barrier between them).  (Measured: asynchronous
+  // global -> shared copies of the region, issued ahead of the step-control
+  // reads, were 11 % slower in binary64 and no faster in binary32.)
   for (int q = threadIdx.x; q < RH * RW; q += blockDim.x) {
     const int r = q / RW, c = q % RW;
     int j = j0 - 2 + r, i = i0 - 2 + c;
@@ -181,7 +231,7 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
       U4[k] = uin[k * plane + (long long)j * pitch + i];
       s.U[k][q] = U4[k];
     }
-    cons_to_prim(U4, W4);
+    k_c2p(U4, W4);
 #pragma unroll
     for (int k = 0; k < NV; k++) s.W[k][q] = W4[k];
   }
@@ -204,7 +254,7 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
       T U4[NV], W4[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) U4[k] = s.U[k][rs * RW + c];
-      cons_to_prim(U4, W4);
+      k_c2p(U4, W4);
 #pragma unroll
       for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
     }
@@ -218,7 +268,7 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
       T U4[NV], W4[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) U4[k] = s.U[k][r * RW + cs];
-      cons_to_prim(U4, W4);
+      k_c2p(U4, W4);
 #pragma unroll
       for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
     }
@@ -231,16 +281,15 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const T* __restrict__ uin,
     const int c = 2 + q % TW, r = 2 + q / TW;
     const int i = i0 + c - 2, j = j0 + r - 2;
     if (i < nx && j < ny) {
-      T U4[NV], W4[NV];
+      T U4[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) {
         U4[k] = s.U[k][r * RW + c];
         uout[k * plane + (long long)j * pitch + i] = U4[k];
       }
-      cons_to_prim(U4, W4);
-      const T cs = sound_speed(W4[3], W4[0]);
-      const unsigned long long sx = speed_bits((double)(std::fabs(W4[1]) + cs));
-      const unsigned long long sy = speed_bits((double)(std::fabs(W4[2]) + cs));
+      T vx, vy;
+      k_speeds(U4, vx, vy);
+      const unsigned long long sx = speed_bits((double)vx), sy = speed_bits((double)vy);
       bx = sx > bx ? sx : bx;
       by = sy > by ? sy : by;
     }
@@ -259,13 +308,12 @@ __global__ void __launch_bounds__(256) speed_kernel(const T* __restrict__ u, int
   unsigned long long bx = 0, by = 0;
   for (long long q = blockIdx.x * 256LL + threadIdx.x; q < (long long)nx * ny; q += (long long)gridDim.x * 256) {
     const int i = (int)(q % nx), j = (int)(q / nx);
-    T U4[NV], W4[NV];
+    T U4[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) U4[k] = u[k * plane + (long long)j * pitch + i];
-    cons_to_prim(U4, W4);
-    const T cs = sound_speed(W4[3], W4[0]);
-    const unsigned long long sx = speed_bits((double)(std::fabs(W4[1]) + cs));
-    const unsigned long long sy = speed_bits((double)(std::fabs(W4[2]) + cs));
+    T vx, vy;
+    k_speeds(U4, vx, vy);
+    const unsigned long long sx = speed_bits((double)vx), sy = speed_bits((double)vy);
     bx = sx > bx ? sx : bx;
     by = sy > by ? sy : by;
   }
