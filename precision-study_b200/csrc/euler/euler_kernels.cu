@@ -112,16 +112,33 @@ struct Tile {
   static constexpr int RH = TY + 4;
   static constexpr int N = RH * RW;  // cells of the region
   T U[NV][N];
-  T W[NV][N];   // primitives; reused for the interface fluxes
-  T HL[NV][N];  // Hancock-evolved left (lower) face of each cell
+  T W[NV][N];   // primitives
+  T HL[NV][N];  // Hancock-evolved left (lower) face of each cell; then the interface fluxes
   T HR[NV][N];  // ... right (upper) face
+};
+
+// Where the last sweep's updated cells go: the output state (interior cells
+// only) and the running maxima of the next step's signal speeds.
+template <class T>
+struct TileOut {
+  T* __restrict__ u;
+  long long plane;
+  int pitch, i0, j0, nx, ny;
+  unsigned long long bx, by;
 };
 
 // One sweep over the region cells [r0, r1) x [c0, c1) that are updated;
 // DIR 0 = x (along c), 1 = y (along r).  Needs W valid on the cells within
-// 2 of them along DIR.
-template <class T, int TY, int DIR, bool HLL>
-__device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, int c1, T fac, T ratio) {
+// 2 of them along DIR.  The update phase also does what follows it: the
+// first sweep (LAST = false) forms the primitives of each updated cell for
+// the second sweep's reconstruction; the last one stores the tile and
+// reduces the signal speeds.  (Region rows or columns beyond a wall hold
+// copies of the edge cells, and a sweep along them gives the edge cell's
+// result bit for bit, so their primitives are the refreshed ghost copies of
+// the reference's applyBC between the sweeps.)
+template <class T, int TY, int DIR, bool HLL, bool LAST>
+__device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, int c1, T fac, T ratio,
+                                      TileOut<T>& out) {
   constexpr int NI = DIR == 0 ? 1 : 2, TI = DIR == 0 ? 2 : 1;
   const int step = DIR == 0 ? 1 : RW;
   // Hancock faces of the cells one beyond the updated ones along DIR.
@@ -142,7 +159,8 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
   }
   __syncthreads();
   // Interface fluxes: F at cell id = flux between id - step and id, for the
-  // updated cells and the one past them.
+  // updated cells and the one past them; stored over HL[id], which only this
+  // thread reads.
   const int fr1 = DIR == 1 ? r1 + 1 : r1, fc1 = DIR == 0 ? c1 + 1 : c1;
   const int fw = fc1 - c0, fn = (fr1 - r0) * fw;
   for (int q = threadIdx.x; q < fn; q += blockDim.x) {
@@ -155,16 +173,37 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
     }
     k_flux<T, NI, TI, HLL>(a, b, f);
 #pragma unroll
-    for (int k = 0; k < NV; k++) s.W[k][id] = f[k];
+    for (int k = 0; k < NV; k++) s.HL[k][id] = f[k];
   }
   __syncthreads();
   const int uw = c1 - c0, un = (r1 - r0) * uw;
   for (int q = threadIdx.x; q < un; q += blockDim.x) {
-    const int id = (r0 + q / uw) * RW + c0 + q % uw;
+    const int r = r0 + q / uw, c = c0 + q % uw, id = r * RW + c;
+    T U4[NV];
 #pragma unroll
-    for (int k = 0; k < NV; k++) s.U[k][id] -= ratio * (s.W[k][id + step] - s.W[k][id]);
+    for (int k = 0; k < NV; k++) U4[k] = s.U[k][id] - ratio * (s.HL[k][id + step] - s.HL[k][id]);
+    if (!LAST) {
+      T W4[NV];
+      k_c2p(U4, W4);
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        s.U[k][id] = U4[k];
+        s.W[k][id] = W4[k];
+      }
+    } else {
+      const int i = out.i0 + c - 2, j = out.j0 + r - 2;
+      if (i < out.nx && j < out.ny) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) out.u[k * out.plane + (long long)j * out.pitch + i] = U4[k];
+        T vx, vy;
+        k_speeds(U4, vx, vy);
+        const unsigned long long sx = speed_bits((double)vx), sy = speed_bits((double)vy);
+        out.bx = sx > out.bx ? sx : out.bx;
+        out.by = sy > out.by ? sy : out.by;
+      }
+    }
   }
-  __syncthreads();
+  if (!LAST) __syncthreads();
 }
 
 // Registers: 64 per thread for 1024 / NT resident CTAs (the shared-memory
@@ -238,63 +277,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) step_kernel(const T* __restrict
   }
   __syncthreads();
   const T facx = (T)0.5 * dt / dx, facy = (T)0.5 * dt / dy, rx = dt / dx, ry = dt / dy;
-  // Rows / columns of the region beyond the walls hold copies of the edge
-  // cells; after the first sweep they are refreshed from the updated edge
-  // (the reference's applyBC between the sweeps).
-  const int rlo = j0 - 2 < 0 ? 2 - j0 : 0, rhi = j0 - 2 + RH > ny ? ny - (j0 - 2) : RH;  // in-domain rows [rlo, rhi)
-  const int clo = i0 - 2 < 0 ? 2 - i0 : 0, chi = i0 - 2 + RW > nx ? nx - (i0 - 2) : RW;
-  // Between the sweeps, a region row (column) beyond a wall holds a copy of
-  // the updated edge row (column); only its primitives are read afterwards,
-  // so they are formed from the edge cell directly.
+  TileOut<T> out{uout, plane, pitch, i0, j0, nx, ny, 0ull, 0ull};
   if (n % 2 == 0) {
-    // x sweep on every region row (columns 2..33), then y sweep on the tile.
-    sweep<T, TY, 0, HLL>(s, 0, RH, 2, TW + 2, facx, rx);
-    for (int q = threadIdx.x; q < RH * TW; q += blockDim.x) {
-      const int r = q / TW, c = 2 + q % TW;
-      const int rs = r < rlo ? rlo : (r >= rhi ? rhi - 1 : r);
-      T U4[NV], W4[NV];
-#pragma unroll
-      for (int k = 0; k < NV; k++) U4[k] = s.U[k][rs * RW + c];
-      k_c2p(U4, W4);
-#pragma unroll
-      for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
-    }
-    __syncthreads();
-    sweep<T, TY, 1, HLL>(s, 2, TY + 2, 2, TW + 2, facy, ry);
+    // x sweep on every region row (columns 2..TW+1), then y sweep on the tile.
+    sweep<T, TY, 0, HLL, false>(s, 0, RH, 2, TW + 2, facx, rx, out);
+    sweep<T, TY, 1, HLL, true>(s, 2, TY + 2, 2, TW + 2, facy, ry, out);
   } else {
-    sweep<T, TY, 1, HLL>(s, 2, TY + 2, 0, RW, facy, ry);
-    for (int q = threadIdx.x; q < TY * RW; q += blockDim.x) {
-      const int r = 2 + q / RW, c = q % RW;
-      const int cs = c < clo ? clo : (c >= chi ? chi - 1 : c);
-      T U4[NV], W4[NV];
-#pragma unroll
-      for (int k = 0; k < NV; k++) U4[k] = s.U[k][r * RW + cs];
-      k_c2p(U4, W4);
-#pragma unroll
-      for (int k = 0; k < NV; k++) s.W[k][r * RW + c] = W4[k];
-    }
-    __syncthreads();
-    sweep<T, TY, 0, HLL>(s, 2, TY + 2, 2, TW + 2, facx, rx);
+    sweep<T, TY, 1, HLL, false>(s, 2, TY + 2, 0, RW, facy, ry, out);
+    sweep<T, TY, 0, HLL, true>(s, 2, TY + 2, 2, TW + 2, facx, rx, out);
   }
-  // Store the tile and reduce the next step's signal speeds.
-  unsigned long long bx = 0, by = 0;
-  for (int q = threadIdx.x; q < TW * TY; q += blockDim.x) {
-    const int c = 2 + q % TW, r = 2 + q / TW;
-    const int i = i0 + c - 2, j = j0 + r - 2;
-    if (i < nx && j < ny) {
-      T U4[NV];
-#pragma unroll
-      for (int k = 0; k < NV; k++) {
-        U4[k] = s.U[k][r * RW + c];
-        uout[k * plane + (long long)j * pitch + i] = U4[k];
-      }
-      T vx, vy;
-      k_speeds(U4, vx, vy);
-      const unsigned long long sx = speed_bits((double)vx), sy = speed_bits((double)vy);
-      bx = sx > bx ? sx : bx;
-      by = sy > by ? sy : by;
-    }
-  }
+  unsigned long long bx = out.bx, by = out.by;
   bx = warp_max(bx);
   by = warp_max(by);
   if ((threadIdx.x & 31) == 0) {
