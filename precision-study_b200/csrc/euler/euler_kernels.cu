@@ -5,7 +5,7 @@
 // that runs a whole 1D Riemann problem (src/euler/riemann1d_cpu.cpp:95-196).
 //
 // 2D step kernel.  A CTA of 512 threads owns a 32 x TY tile of output cells
-// (TY = 16 fp64, 32 fp32).  It loads the conservative state of a
+// (TY = 16 or 12 fp64, 32 fp32).  It loads the conservative state of a
 // (TY + 4) x 36 region around it (2 cells of halo,
 // indices clamped at the walls: the reference's transmissive ghost copies,
 // riemann2d_cpu.cpp:160-182), and runs the first sweep on the part of the
@@ -208,8 +208,8 @@ __device__ __forceinline__ void sweep(Tile<T, TY>& s, int r0, int r1, int c0, in
 
 // Registers: 64 per thread for 1024 / NT resident CTAs (the shared-memory
 // limit of the tile shapes below).
-template <class T, int TY, int NT, bool HLL>
-__global__ void __launch_bounds__(NT, 1024 / NT) step_kernel(const T* __restrict__ uin, T* __restrict__ uout, int nx, int ny,
+template <class T, int TY, int NT, int MINB, bool HLL>
+__global__ void __launch_bounds__(NT, MINB) step_kernel(const T* __restrict__ uin, T* __restrict__ uout, int nx, int ny,
                                                    int pitch, long long plane, T dx, T dy, T cfl, EulerCtrl* ctrl,
                                                    int p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -400,10 +400,10 @@ __global__ void __launch_bounds__(1024) riemann1d_kernel(T* __restrict__ u, T* _
   }
 }
 
-template <class T, int TY, int NT, bool HLL>
+template <class T, int TY, int NT, int MINB, bool HLL>
 cudaError_t launch_step(const void* uin, void* uout, int nx, int ny, int pitch, long long plane, double dx, double dy,
                         double cfl, EulerCtrl* ctrl, int p, cudaStream_t s) {
-  auto k = step_kernel<T, TY, NT, HLL>;  // shared-memory limit set by prepare()
+  auto k = step_kernel<T, TY, NT, MINB, HLL>;  // shared-memory limit set by prepare()
   const size_t smem = sizeof(Tile<T, TY>);
   const dim3 grid((nx + TW - 1) / TW, (ny + TY - 1) / TY);
   k<<<grid, NT, smem, s>>>(static_cast<const T*>(uin), static_cast<T*>(uout), nx, ny, pitch, plane, (T)dx, (T)dy,
@@ -411,21 +411,21 @@ cudaError_t launch_step(const void* uin, void* uout, int nx, int ny, int pitch, 
   return cudaGetLastError();
 }
 
-template <class T, int TY, int NT>
+template <class T, int TY, int NT, int MINB>
 cudaError_t allow_smem() {
-  cudaError_t e = cudaFuncSetAttribute(step_kernel<T, TY, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(Tile<T, TY>));
+  cudaError_t e = cudaFuncSetAttribute(step_kernel<T, TY, NT, MINB, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Tile<T, TY>));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(step_kernel<T, TY, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(step_kernel<T, TY, NT, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(Tile<T, TY>));
   return e;
 }
 
-template <class T, int TY, int NT>
+template <class T, int TY, int NT, int MINB>
 cudaError_t launch_any(int hll, const void* uin, void* uout, int nx, int ny, int pitch, long long plane, double dx,
                        double dy, double cfl, EulerCtrl* ctrl, int p, cudaStream_t s) {
-  return hll ? launch_step<T, TY, NT, true>(uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s)
-             : launch_step<T, TY, NT, false>(uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
+  return hll ? launch_step<T, TY, NT, MINB, true>(uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s)
+             : launch_step<T, TY, NT, MINB, false>(uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
 }
 
 }  // namespace
@@ -434,22 +434,28 @@ cudaError_t launch_any(int hll, const void* uin, void* uout, int nx, int ny, int
 // and 32 x 32 for fp32, 512 threads, two CTAs (32 warps) per SM at 64
 // registers (shared memory: 92 KB / 83 KB for the four region arrays).
 // Against 32 x 8 (fp64) / 32 x 16 (fp32) tiles of 256 threads at four CTAs
-// per SM, the same occupancy with less halo re-work and half the block
-// barriers per cell: fp64 10.06 -> 11.56 G, fp32 21.4 -> 25.1 G
-// zone-cycles/s.  (With 256 threads, 16 rows in fp64 held only 16 warps per
-// SM and were 10 % slower than 8.)
-constexpr int kTY64 = 16, kTY32 = 32, kThreads = 512;
+// per SM: the same occupancy with less halo re-work and half the block
+// barriers per cell (fp64 +15 %, fp32 +17 %).  Measured and not kept at
+// 4096^2: fp64 32 x 12 (-6 %), fp32 32 x 28 / 32 x 24 at three CTAs per SM
+// (-13 % / -20 %).  fp64 grids whose 32 x 16 tiling fills less than one wave
+// of two CTAs per SM take 32 x 12 tiles (the 500 x 197 shock-bubble: 46.1 ->
+// 41.3 ms).
+constexpr int kThreads = 512;
 
 cudaError_t prepare() {
-  cudaError_t e = allow_smem<double, kTY64, kThreads>();
-  if (e == cudaSuccess) e = allow_smem<float, kTY32, kThreads>();
+  cudaError_t e = allow_smem<double, 16, kThreads, 2>();
+  if (e == cudaSuccess) e = allow_smem<double, 12, kThreads, 2>();
+  if (e == cudaSuccess) e = allow_smem<float, 32, kThreads, 2>();
   return e;
 }
 
 cudaError_t step2d(int fp32, int hll, const void* uin, void* uout, int nx, int ny, int pitch, long long plane,
                    double dx, double dy, double cfl, EulerCtrl* ctrl, int p, cudaStream_t s) {
-  if (fp32) return launch_any<float, kTY32, kThreads>(hll, uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
-  return launch_any<double, kTY64, kThreads>(hll, uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
+  if (fp32) return launch_any<float, 32, kThreads, 2>(hll, uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
+  const long long tiles16 = (long long)((nx + TW - 1) / TW) * ((ny + 15) / 16);
+  if (tiles16 < 2 * 148)
+    return launch_any<double, 12, kThreads, 2>(hll, uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
+  return launch_any<double, 16, kThreads, 2>(hll, uin, uout, nx, ny, pitch, plane, dx, dy, cfl, ctrl, p, s);
 }
 
 cudaError_t speed2d(int fp32, const void* u, int nx, int ny, int pitch, long long plane, EulerCtrl* ctrl, int slot,

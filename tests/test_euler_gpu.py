@@ -47,6 +47,16 @@ def test_2d_exact_rectangular_grids_match_the_oracle(oracle, pmhd_lib, shape, pr
         np.testing.assert_array_equal(e.prims(), ref)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_2d_exact_large_grid_matches_the_oracle(oracle, pmhd_lib, prec):
+    """640 x 480: enough tiles for the binary64 kernel's 32 x 16 tile shape
+    (smaller grids take 32 x 12 tiles); 20 steps, both step orders."""
+    steps, t, ref = EL.riemann2d(640, 6, "hllc", prec, ny=480, max_steps=20)
+    with pmhd_lib.Euler2D(640, 480, config=6, precision=prec, exact=True) as e:
+        assert e.advance(max_steps=20).steps == steps == 20
+        np.testing.assert_array_equal(e.prims(), ref)
+
+
 def test_2d_step_limited_runs_resume_exactly(oracle, pmhd_lib):
     steps, t, ref = EL.riemann2d(80, 12, "hllc", "fp64")
     _, _, ref7 = EL.riemann2d(80, 12, "hllc", "fp64", max_steps=7)
