@@ -542,9 +542,9 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, ma
                       precision=precision) as L:
         out["relax"], out["train_noise"] = L.cfg.relax, L.cfg.train_noise
         t0 = time.perf_counter()
-        for prob, par in train:
-            L.generate(prob, par, t_end=t_end, every=every)
+        per_run = [L.generate(prob, par, t_end=t_end, every=every) for prob, par in train]
         t1 = time.perf_counter()
+        out["pairs_per_training_run"] = per_run
         losses = L.train(iters=iters, batch=8, lr=2e-3)
         t2 = time.perf_counter()
         out.update({"pairs": L.num_pairs, "generate_s": t1 - t0, "train_s": t2 - t1, "train_iters": iters,
@@ -766,8 +766,11 @@ def main():
         if args.learned >= 128:
             # BASELINE's configuration: 2048^2 fine -> 512^2 coarse, OT and KH
             # states, fine runs in binary64.
+            # One pair every n / 16 coarse steps and room for 640 pairs: about 80
+            # pairs from each of the eight training runs (at n / 32 and 600 the
+            # four Orszag-Tang runs filled the store before any KH run).
             learned[f"coarse_{args.learned}"] = bench_learned(
-                pmhd, args.learned, local, iters=1000, every=max(1, args.learned // 32), max_pairs=600, kh=True,
+                pmhd, args.learned, local, iters=1000, every=max(1, args.learned // 16), max_pairs=640, kh=True,
                 precision="fp64")
 
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------

@@ -321,6 +321,9 @@ typedef struct {
                                  into an unstable run)                         */
   double train_noise;         /* std of Gaussian noise added to the normalised
                                  network inputs in training (0.03; 0: none)   */
+  double shrink;              /* soft threshold on the normalised network
+                                 outputs: only the part beyond +-shrink is
+                                 applied (0: all of it)                        */
 } pmhd_learned_config;
 
 typedef struct {

@@ -150,7 +150,7 @@ struct CorrBuffers {
     ok = ok && grab(dalloc(&cs.a1, (size_t)pix * kWidth), cs.a1) && grab(dalloc(&cs.z2, (size_t)pix * kWidth), cs.z2);
     ok = ok && grab(dalloc(&cs.a2, (size_t)pix * kWidth), cs.a2) && grab(dalloc(&cs.out, (size_t)pix * kOut), cs.out);
     ok = ok && grab(dalloc(&cs.z3, (size_t)pix * kWidth), cs.z3) && grab(dalloc(&cs.a3, (size_t)pix * kWidth), cs.a3);
-    ok = ok && grab(dalloc(&cs.flags, 4), cs.flags) && grab(dalloc(&cs.sums, 4), cs.sums);
+    ok = ok && grab(dalloc(&cs.flags, 4), cs.flags) && grab(dalloc(&cs.sums, kCorrSums), cs.sums);
     ok = ok && grab(dalloc(&cs.counters, 4), cs.counters) && grab(dalloc(&cs.accept, 4), cs.accept);
     if (!ok) {
       cudaGetLastError();
@@ -158,8 +158,9 @@ struct CorrBuffers {
     }
     cs.norm = L->dnorm;
     cs.relax = L->cfg.relax;
+    cs.shrink = L->cfg.shrink;
     cudaError_t e = cudaMemsetAsync(cs.flags, 0, 4 * sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(cs.sums, 0, 4 * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cs.sums, 0, kCorrSums * sizeof(double), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(cs.counters, 0, 4 * sizeof(unsigned long long), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e == cudaSuccess ? PMHD_OK : PMHD_ERR_CUDA;
@@ -213,6 +214,7 @@ int pmhd_learned_config_default(pmhd_learned_config* c) {
   c->div_tol = 0.5;
   c->relax = 0.25;
   c->train_noise = 0.03;
+  c->shrink = 0.0;
   return PMHD_OK;
 }
 
@@ -238,7 +240,8 @@ int pmhd_learned_create(const pmhd_learned_config* cfg, pmhd_learned** out) {
   if (!cfg || cfg->nx < 8 || cfg->ny < 8 || cfg->refine < 2 || cfg->refine > 16 || cfg->max_pairs < 1 ||
       !(cfg->x_max > cfg->x_min) || !(cfg->y_max > cfg->y_min) || !(cfg->gamma > 1.0) || !(cfg->cfl > 0.0) ||
       !(cfg->cfl < 1.0) || !(cfg->alpha > 0.0) || !(cfg->div_tol >= 0.0) ||
-      !(cfg->relax >= 0.0) || !(cfg->relax <= 1.0) || !(cfg->train_noise >= 0.0))
+      !(cfg->relax >= 0.0) || !(cfg->relax <= 1.0) || !(cfg->train_noise >= 0.0) ||
+      !(cfg->shrink >= 0.0))
     return PMHD_ERR_ARG;
   if (cfg->precision != PMHD_FP64 && cfg->precision != PMHD_MIXED) return PMHD_ERR_UNSUPPORTED;
   int ndev = 0;

@@ -337,15 +337,22 @@ __global__ void store_interior_kernel(const double* __restrict__ u, int pitch, l
 // Candidate = the state after the step corrected by the network output:
 // density and pressure scaled by exp(correction) (the exponent clamped to
 // [-2, 2]), velocities, B_z and psi shifted, B_x and B_y shifted by the
-// central-difference curl of the potential (periodic); flags a cell whose
-// density or pressure is not positive (or not finite).
+// central-difference curl of the potential (periodic).  Accumulates the
+// domain sums of the changes of the conserved quantities (sums[2..]).
+__constant__ int kConserved[kNConserved] = {0, 1, 2, 3, 4, 7};
+
 __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long long plane, int nx, int ny,
                                  const float* __restrict__ out, const Norm* __restrict__ norm, double gamma,
-                                 double dx, double dy, double relax, double* __restrict__ cand,
-                                 int* __restrict__ flags, const Ctrl* __restrict__ c, int p) {
+                                 double dx, double dy, double relax, double shrink, double* __restrict__ cand,
+                                 double* __restrict__ sums, const Ctrl* __restrict__ c, int p) {
   if (!step_taken(c, p)) return;
   const long long n = (long long)nx * ny;
-  int bad = 0;
+  double dsum[kNConserved] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // Soft threshold: sign(o) max(|o| - shrink, 0) of a normalised output.
+  auto shr = [shrink](float o) {
+    const double a = fabs((double)o) - shrink;
+    return a > 0.0 ? copysign(a, (double)o) : 0.0;
+  };
   const double sA = relax * norm->sig_out[OUT_A];
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % nx), j = (int)(q / nx);
@@ -353,7 +360,7 @@ __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long l
 #pragma unroll
     for (int k = 0; k < kNVar; k++) U[k] = u[k * plane + (long long)(j + 2) * pitch + (i + 2)];
     const float* o = out + q * kOut;
-    auto sig = [&](int k) { return relax * (double)norm->sig_out[k] * (double)o[k]; };
+    auto sig = [&](int k) { return relax * (double)norm->sig_out[k] * shr(o[k]); };
     auto clamp2 = [](double x) { return x < -2.0 ? -2.0 : (x > 2.0 ? 2.0 : x); };
     const double rho = U[0], inv = 1.0 / rho;
     const double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
@@ -363,8 +370,10 @@ __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long l
     const double vx1 = vx + sig(OUT_V), vy1 = vy + sig(OUT_V + 1), vz1 = vz + sig(OUT_V + 2);
     const double p1 = pr * exp(clamp2(sig(OUT_LP)));
     const int ip = (i + 1) % nx, im = (i + nx - 1) % nx, jp = (j + 1) % ny, jm = (j + ny - 1) % ny;
-    const double a_n = sA * out[((long long)jp * nx + i) * kOut + OUT_A], a_s = sA * out[((long long)jm * nx + i) * kOut + OUT_A];
-    const double a_e = sA * out[((long long)j * nx + ip) * kOut + OUT_A], a_w = sA * out[((long long)j * nx + im) * kOut + OUT_A];
+    const double a_n = sA * shr(out[((long long)jp * nx + i) * kOut + OUT_A]);
+    const double a_s = sA * shr(out[((long long)jm * nx + i) * kOut + OUT_A]);
+    const double a_e = sA * shr(out[((long long)j * nx + ip) * kOut + OUT_A]);
+    const double a_w = sA * shr(out[((long long)j * nx + im) * kOut + OUT_A]);
     const double bx1 = U[5] + (a_n - a_s) / (2.0 * dy), by1 = U[6] - (a_e - a_w) / (2.0 * dx);
     const double bz1 = U[7] + sig(OUT_BZ), psi1 = U[8] + sig(OUT_PSI);
     double* C = cand + q * kNVar;
@@ -378,7 +387,39 @@ __global__ void candidate_kernel(const double* __restrict__ u, int pitch, long l
     C[6] = by1;
     C[7] = bz1;
     C[8] = psi1;
-    if (!(rho1 > 0.0) || !(p1 > 0.0) || !isfinite(C[4]) || !isfinite(C[1] + C[2] + C[3] + C[5] + C[6] + C[8]))
+#pragma unroll
+    for (int k = 0; k < kNConserved; k++) dsum[k] += C[kConserved[k]] - U[kConserved[k]];
+  }
+#pragma unroll
+  for (int k = 0; k < kNConserved; k++) {
+    double v = dsum[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sums[2 + k], v);
+  }
+}
+
+// The restricted fine state and the coarse state conserve the same totals on
+// the periodic grid, so the true correction of a conserved quantity has zero
+// mean: its domain mean is removed from the candidate (a systematic bias of
+// the network would otherwise build up step after step).  Then flags a cell
+// whose density or pressure is not positive (or not finite).
+__global__ void conserve_kernel(double* __restrict__ cand, int nx, int ny, double gamma,
+                                const double* __restrict__ sums, int* __restrict__ flags,
+                                const Ctrl* __restrict__ c, int p) {
+  if (!step_taken(c, p)) return;
+  const long long n = (long long)nx * ny;
+  double mean[kNConserved];
+#pragma unroll
+  for (int k = 0; k < kNConserved; k++) mean[k] = sums[2 + k] / (double)n;
+  int bad = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    double* C = cand + q * kNVar;
+#pragma unroll
+    for (int k = 0; k < kNConserved; k++) C[kConserved[k]] -= mean[k];
+    const double rho = C[0];
+    const double pr = (gamma - 1.0) * (C[4] - 0.5 * (C[1] * C[1] + C[2] * C[2] + C[3] * C[3]) / rho -
+                                       0.5 * (C[5] * C[5] + C[6] * C[6] + C[7] * C[7]));
+    if (!(rho > 0.0) || !(pr > 0.0) || !isfinite(C[4]) || !isfinite(C[1] + C[2] + C[3] + C[5] + C[6] + C[8]))
       bad = 1;
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1);
@@ -429,7 +470,7 @@ __global__ void decide_kernel(int* __restrict__ flags, double* __restrict__ sums
   }
   *accept = acc;
   flags[0] = 0;
-  sums[0] = sums[1] = 0.0;
+  for (int k = 0; k < kCorrSums; k++) sums[k] = 0.0;
 }
 
 __global__ void commit_kernel(const double* __restrict__ cand, double* __restrict__ u, int pitch, long long plane,
@@ -539,9 +580,11 @@ cudaError_t correct_step(const CorrState& cs, void* u, int pitch, long long plan
   double* ud = static_cast<double*>(u);
   const long long n = (long long)nx * ny;
   candidate_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.out, cs.norm, gamma, dx, dy,
-                                                    cs.relax, cs.cand, cs.flags, ctrl, p);
+                                                    cs.relax, cs.shrink, cs.cand, cs.sums, ctrl, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  conserve_kernel<<<grid_for(n, 256), 256, 0, s>>>(cs.cand, nx, ny, gamma, cs.sums, cs.flags, ctrl, p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   divnorm_kernel<<<grid_for(n, 256), 256, 0, s>>>(ud, pitch, plane, nx, ny, cs.cand, dx, dy, cs.sums, ctrl, p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   decide_kernel<<<1, 1, 0, s>>>(cs.flags, cs.sums, div_tol, cs.counters, cs.accept, ctrl_w, p);

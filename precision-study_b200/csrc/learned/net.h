@@ -72,6 +72,12 @@ struct NetWeights {
 };
 
 // Per-step work of a corrected run.
+// Conserved quantities whose correction is made mean-free over the periodic
+// grid: rho, the three momenta, E, B_z (B_x and B_y change by a curl, whose
+// mean is zero already).
+constexpr int kNConserved = 6;
+constexpr int kCorrSums = 2 + kNConserved;
+
 struct CorrState {
   double* before;      // SoA copy of the state before the step (solver layout)
   double* cand;        // AoS interior candidate state
@@ -79,14 +85,17 @@ struct CorrState {
   __nv_bfloat16* z1, *a1, *z2, *a2, *z3, *a3;
   float* out;          // network output [ny][nx][16]
   // flags[0]: candidate not positive; sums[0..1]: ||divB||_1 after the step
-  // and of the candidate; counters[0..2]: accepted, rejected (positivity),
-  // rejected (divergence); accept: this step's decision.
+  // and of the candidate, sums[2 + k]: domain sum of the candidate's change
+  // of conserved quantity kConserved[k] (kCorrSums doubles); counters[0..2]:
+  // accepted, rejected (positivity), rejected (divergence); accept: this
+  // step's decision.
   int* flags;
   double* sums;
   unsigned long long* counters;
   int* accept;
   const Norm* norm;    // device copy
   double relax;        // fraction of the predicted correction applied
+  double shrink;       // soft threshold on the normalised outputs
 };
 
 cudaError_t features(const StateView& after, const StateView& before, int batch, int nx, int ny, const Norm* norm,

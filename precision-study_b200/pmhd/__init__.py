@@ -114,7 +114,7 @@ class LearnedConfig(ctypes.Structure):
         ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("alpha", ctypes.c_double),
         ("precision", ctypes.c_int), ("device", ctypes.c_int), ("max_pairs", ctypes.c_int),
         ("seed", ctypes.c_ulonglong), ("div_tol", ctypes.c_double), ("relax", ctypes.c_double),
-        ("train_noise", ctypes.c_double),
+        ("train_noise", ctypes.c_double), ("shrink", ctypes.c_double),
     ]
 
 

@@ -278,6 +278,16 @@ def test_learned_correction_trains_and_beats_the_plain_coarse_grid(pmhd_lib, tmp
         print(f"relL2 vs restricted fine: rho plain {rho_p:.4e} corrected {rho_c:.4e}; mean plain {mean_p:.4e} "
               f"corrected {mean_c:.4e}; accepted {sc.accepted}/{sc.steps}")
         assert rho_c < rho_p and mean_c < mean_p
+        # The corrections of the conserved quantities are mean-free: the
+        # corrected run keeps the periodic totals of rho, momentum and B_z that
+        # the plain run keeps, to the rounding drift of the solver itself (the
+        # plain run's x-momentum total moves by ~1e-8 over these 314 steps;
+        # an uncorrected bias of the network would move them by orders of
+        # magnitude more).  (E is left out: the GLM coupling makes its total
+        # depend on the trajectory.)
+        for k in (0, 1, 2, 3, 7):
+            tc, tp = corr[..., k].sum(), plain[..., k].sum()
+            assert abs(tc - tp) <= 1e-9 * np.abs(plain[..., k]).sum(), (k, tc, tp)
         # Weights and normalisation survive a save / load into a new handle.
         path = str(tmp_path / "net.bin")
         L.save(path)

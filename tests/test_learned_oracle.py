@@ -69,7 +69,12 @@ def test_learned_config_defaults_and_argument_checks(pmhd_lib):
     c = pmhd_lib.LearnedConfig()
     assert pmhd_lib.load().pmhd_learned_config_default(ctypes.byref(c)) == pmhd_lib.OK
     assert (c.nx, c.ny, c.refine, c.precision, c.max_pairs) == (64, 64, 4, pmhd_lib.MIXED, 512)
+    assert (c.relax, c.train_noise, c.shrink) == (0.25, 0.03, 0.0)
     h = ctypes.c_void_p(1)
+    bad = pmhd_lib.LearnedConfig.from_buffer_copy(c)
+    bad.shrink = -0.5
+    assert pmhd_lib.load().pmhd_learned_create(ctypes.byref(bad), ctypes.byref(h)) == pmhd_lib.ERR_ARG
+    assert h.value is None
     bad = pmhd_lib.LearnedConfig.from_buffer_copy(c)
     bad.refine = 1
     assert pmhd_lib.load().pmhd_learned_create(ctypes.byref(bad), ctypes.byref(h)) == pmhd_lib.ERR_ARG
