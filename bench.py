@@ -511,7 +511,7 @@ def bench_shock_bubble(pmhd, device, max_over_ranks, world, reference_gpu=True):
 
 
 def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, max_pairs=1500, seed=11,
-                  kh=False, precision="mixed"):
+                  kh=False, precision="mixed", shrinks=(0.0,)):
     """Learned correction: training pairs from the solver (Orszag-Tang with
     the field scaled by B0 in {0.7, 0.85, 1.15, 1.3}; with kh, also the
     periodic Kelvin-Helmholtz double shear layer with widths {0.03, 0.045,
@@ -519,7 +519,9 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, ma
     the held-out B0 = 1 (and width 0.055).  Errors are relative L2 (rho, the
     mean over rho, mx, my, E, Bx, By, and all values at once) against the fine
     run restricted to the coarse grid; wall times are those of the time
-    loops; the corrected run's speed-up is against the fine run's wall."""
+    loops; the corrected run's speed-up is against the fine run's wall.  Each
+    value in `shrinks` beyond the first adds a corrected run with that soft
+    threshold on the network outputs (same weights)."""
     import numpy as np
     OT, KH = pmhd.PROBLEM_ORSZAG_TANG, pmhd.PROBLEM_KH_REF
     live = [0, 1, 2, 4, 5, 6]
@@ -570,6 +572,21 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, ma
                 rec["gain"] = {k: rec["relL2_vs_fine"]["learned_coarse"][k] < rec["relL2_vs_fine"]["plain_coarse"][k]
                                for k in ("rho", "mean", "all")}
             out[name] = rec
+        if len(shrinks) > 1:
+            path = os.path.join(tempfile.mkdtemp(), "net.bin")
+            L.save(path)
+            for sh in shrinks[1:]:
+                with pmhd.Learned(nx=n, ny=n, refine=refine, max_pairs=1, seed=seed, device=device,
+                                  precision=precision, shrink=sh) as L2:
+                    L2.load_weights(path)
+                    for name, (prob, par) in tests.items():
+                        key = f"learned_coarse_shrink_{sh:g}"
+                        try:
+                            corr, sc = L2.run(prob, par, t_end=t_end, use_net=True)
+                            fine, _ = L.fine_run(prob, par, t_end=t_end, refine=refine)
+                            out[name]["relL2_vs_fine"][key] = err(corr, fine)
+                        except pmhd.PmhdError as exc:
+                            out[name][key] = f"failed: {exc}"
     return out
 
 
@@ -771,7 +788,7 @@ def main():
             # four Orszag-Tang runs filled the store before any KH run).
             learned[f"coarse_{args.learned}"] = bench_learned(
                 pmhd, args.learned, local, iters=1000, every=max(1, args.learned // 16), max_pairs=640, kh=True,
-                precision="fp64")
+                precision="fp64", shrinks=(0.0, 1.0))
 
     # ---- CPU baseline: the reference serial solver, rank 0 at N = 1 ----------
     cpu = None

@@ -436,8 +436,8 @@ cudaError_t launch_any(int hll, const void* uin, void* uout, int nx, int ny, int
 // Against 32 x 8 (fp64) / 32 x 16 (fp32) tiles of 256 threads at four CTAs
 // per SM: the same occupancy with less halo re-work and half the block
 // barriers per cell (fp64 +15 %, fp32 +17 %).  Measured and not kept at
-// 4096^2: fp64 32 x 12 (-6 %), fp32 32 x 28 / 32 x 24 at three CTAs per SM
-// (-13 % / -20 %).  fp64 grids whose 32 x 16 tiling fills less than one wave
+// 4096^2: fp64 32 x 12 (-6 %), fp64 32 x 10 with 320 threads at three CTAs
+// per SM (-18 %), fp32 32 x 28 / 32 x 24 at three CTAs per SM (-13 % / -20 %).  fp64 grids whose 32 x 16 tiling fills less than one wave
 // of two CTAs per SM take 32 x 12 tiles (the 500 x 197 shock-bubble: 46.1 ->
 // 41.3 ms).
 constexpr int kThreads = 512;
