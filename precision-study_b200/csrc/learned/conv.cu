@@ -6,10 +6,13 @@
 // from are periodic).  Weights are [c_out][9][c_in] with tap t = (dy+1)*3 +
 // (dx+1): out(y, x) = sum_t W[t] x(y+dy, x+dx) (cross-correlation).
 //
-// Implicit GEMM.  Forward / backward-data: one CTA computes 128 output
-// pixels (M = 128) x c_out channels (N); K = 9 taps x c_in channels.  The
-// CTA gathers the 9 shifted copies of its pixels' input vectors (periodic
-// wrap) into K-major shared-memory tiles, one thread issues 9 * c_in / 16
+// Implicit GEMM.  Forward / backward-data: M = 128 output pixels x N = c_out
+// channels, K = 9 taps x c_in channels.  Row kernel (width a multiple of
+// 128, height of 8): the CTA stages its rows' input once, each tap's operand
+// is a shifted descriptor into it, one thread issues 8 rows x 9 * c_in / 16
+// tcgen05.mma, eight warps run the epilogue.  Gather kernel (other shapes):
+// one CTA per 128 pixels gathers the 9 shifted copies of its pixels' input
+// vectors (periodic wrap) into K-major tiles, one thread issues 9 * c_in / 16
 // tcgen05.mma, the four warps read the 128 x N accumulator back with
 // tcgen05.ld and run the epilogue.  Weight gradient: D[(t, c_in)][c_out] =
 // sum over pixels of x(p + tap) dz(p)^T, K = pixels: blocks of 8 pixels x 8
@@ -64,6 +67,52 @@ __device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t parity, int* er
     mbar_wait_bounded(bar, parity, kWaitPolls);
   }
   return ok;
+}
+
+// Epilogue of one output pixel p from its CO fp32 accumulators.
+template <int CO, int EPI>
+__device__ __forceinline__ void epilogue(const float (&acc)[CO], long long p, const float* __restrict__ bias,
+                                         const __nv_bfloat16* __restrict__ zprev, void* __restrict__ out0,
+                                         void* __restrict__ out1) {
+  if (EPI == CONV_GELU) {
+    __nv_bfloat16* z = static_cast<__nv_bfloat16*>(out0) + p * CO;
+    __nv_bfloat16* a = static_cast<__nv_bfloat16*>(out1) + p * CO;
+#pragma unroll
+    for (int c8 = 0; c8 < CO / 8; c8++) {
+      __align__(16) __nv_bfloat16 zb[8], ab[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const float zz = acc[c8 * 8 + q] + bias[c8 * 8 + q];
+        zb[q] = __float2bfloat16_rn(zz);
+        ab[q] = __float2bfloat16_rn(gelu(zz));
+      }
+      *reinterpret_cast<uint4*>(z + c8 * 8) = *reinterpret_cast<const uint4*>(zb);
+      *reinterpret_cast<uint4*>(a + c8 * 8) = *reinterpret_cast<const uint4*>(ab);
+    }
+  } else if (EPI == CONV_LINEAR) {
+    float* o = static_cast<float*>(out0) + p * CO;
+#pragma unroll
+    for (int c4 = 0; c4 < CO / 4; c4++) {
+      float4 v;
+      v.x = acc[c4 * 4 + 0] + bias[c4 * 4 + 0];
+      v.y = acc[c4 * 4 + 1] + bias[c4 * 4 + 1];
+      v.z = acc[c4 * 4 + 2] + bias[c4 * 4 + 2];
+      v.w = acc[c4 * 4 + 3] + bias[c4 * 4 + 3];
+      *reinterpret_cast<float4*>(o + c4 * 4) = v;
+    }
+  } else {
+    const __nv_bfloat16* zp = zprev + p * CO;
+    __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + p * CO;
+#pragma unroll
+    for (int c8 = 0; c8 < CO / 8; c8++) {
+      const uint4 zv = *reinterpret_cast<const uint4*>(zp + c8 * 8);
+      const __nv_bfloat16* zs = reinterpret_cast<const __nv_bfloat16*>(&zv);
+      __align__(16) __nv_bfloat16 db[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) db[q] = __float2bfloat16_rn(acc[c8 * 8 + q] * gelu_grad(__bfloat162float(zs[q])));
+      *reinterpret_cast<uint4*>(d + c8 * 8) = *reinterpret_cast<const uint4*>(db);
+    }
+  }
 }
 
 template <int CG, int CO>
@@ -162,46 +211,135 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
 #pragma unroll
     for (int c8 = 0; c8 < CO / 8; c8++) umma::ld8(tmem + ((uint32_t)(warp * 32) << 16) + c8 * 8, acc + c8 * 8);
     const long long p = p0 + tid;
-    if (p < P) {
-      if (EPI == CONV_GELU) {
-        __nv_bfloat16* z = static_cast<__nv_bfloat16*>(out0) + p * CO;
-        __nv_bfloat16* a = static_cast<__nv_bfloat16*>(out1) + p * CO;
-#pragma unroll
-        for (int c8 = 0; c8 < CO / 8; c8++) {
-          __align__(16) __nv_bfloat16 zb[8], ab[8];
-#pragma unroll
-          for (int q = 0; q < 8; q++) {
-            const float zz = acc[c8 * 8 + q] + bias[c8 * 8 + q];
-            zb[q] = __float2bfloat16_rn(zz);
-            ab[q] = __float2bfloat16_rn(gelu(zz));
-          }
-          *reinterpret_cast<uint4*>(z + c8 * 8) = *reinterpret_cast<const uint4*>(zb);
-          *reinterpret_cast<uint4*>(a + c8 * 8) = *reinterpret_cast<const uint4*>(ab);
+    if (p < P) epilogue<CO, EPI>(acc, p, bias, zprev, out0, out1);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, kCols);
+  }
+}
+
+// Row kernel (forward / backward-data when the width is a multiple of 128
+// and the height of 8): a CTA of 8 warps computes kRows image rows x 128
+// pixels.  It stages the (kRows + 2) x 130 input pixels around them once
+// (periodic wrap), channel-group-interleaved: group g of 8 channels at
+// g * kLboA, then row, then pixel at 16 bytes -- the K-major no-swizzle
+// layout of an M = 128 operand whose rows are pixels.  The operand of tap
+// (dy, dx) for output row r is then the same tile seen from pixel (1 + dx)
+// of staged row (r + 1 + dy): a shift of the descriptor's start address, so
+// the nine taps need no copies.  Accumulators: 128 lanes x CO columns per
+// row, kRows rows side by side in tensor memory.
+constexpr int kRowPix = 128;               // output pixels of a row segment (M)
+constexpr int kRows = 8;                   // output rows per CTA
+constexpr int kRowPitch = kRowPix + 2;     // staged pixels per input row
+constexpr int kRowThreads = 256;
+
+template <int CG, int CO>
+struct RowSmem {
+  static constexpr int K = 9 * CG;
+  static constexpr uint32_t kLboA = (uint32_t)(kRows + 2) * kRowPitch * 16u;  // channel-group stride of A
+  static constexpr uint32_t kBytesA = (uint32_t)(CG / 8) * kLboA;
+  static constexpr uint32_t kOffB = (kBytesA + 127u) & ~127u;
+  static constexpr uint32_t kBytesB = (uint32_t)CO * K * 2u;
+  static constexpr uint32_t kLboB = (uint32_t)CO * 16u;
+  static constexpr uint32_t kOffBar = kOffB + kBytesB;
+  static constexpr uint32_t kBytes = kOffBar + 16u;
+  // Shared memory requested per CTA: at least enough that no more CTAs fit
+  // on an SM than its 512 tensor-memory columns hold (256 columns: two).
+  static constexpr uint32_t kTmemCols = umma::tmem_cols(kRows * CO);
+  static constexpr uint32_t kMinBytes = kTmemCols >= 256u ? 80u * 1024u : 0u;
+  static constexpr uint32_t kLaunchBytes = kBytes > kMinBytes ? kBytes : kMinBytes;
+};
+
+template <int CG, int CO, int EPI>
+__global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                   const __nv_bfloat16* __restrict__ wt,
+                                                                   const float* __restrict__ bias,
+                                                                   const __nv_bfloat16* __restrict__ zprev,
+                                                                   int batch, int h, int w,
+                                                                   void* __restrict__ out0, void* __restrict__ out1,
+                                                                   int* __restrict__ err) {
+  using S = RowSmem<CG, CO>;
+  constexpr uint32_t kCols = S::kTmemCols;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + S::kOffB;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int segs = w / kRowPix, rblocks = h / kRows;
+  const int seg = (int)(blockIdx.x % segs);
+  const int rb = (int)((blockIdx.x / segs) % rblocks);
+  const long long b = blockIdx.x / ((long long)segs * rblocks);
+  const int x0 = seg * kRowPix, y0 = rb * kRows;
+  (void)batch;
+
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  // B operand: weights, row n, K-groups of 8 (16-byte vectors).
+  for (int c = tid; c < CO * (S::K / 8); c += kRowThreads) {
+    const int n = c / (S::K / 8), g = c - n * (S::K / 8);
+    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * S::K + g * 8);
+    *reinterpret_cast<uint4*>(sB + n * 16 + g * S::kLboB) = v;
+  }
+  // A operand: input rows y0 - 1 .. y0 + kRows, pixels x0 - 1 .. x0 + 128
+  // (periodic), one 16-byte channel group per item; consecutive items are
+  // consecutive 16-byte words of the NHWC input.
+  for (int c = tid; c < (kRows + 2) * kRowPitch * (CG / 8); c += kRowThreads) {
+    const int g = c % (CG / 8);
+    const int px = (c / (CG / 8)) % kRowPitch;
+    const int r = c / ((CG / 8) * kRowPitch);
+    const int yy = wrap(y0 - 1 + r, h), xx = wrap(x0 - 1 + px, w);
+    const uint4 v = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CG + g * 8);
+    *reinterpret_cast<uint4*>(sA + g * S::kLboA + (r * kRowPitch + px) * 16) = v;
+  }
+  fence_proxy_async_smem();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {
+    constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll 1
+    for (int r = 0; r < kRows; r++)
+#pragma unroll 1
+      for (int t = 0; t < 9; t++) {
+        int dy = t / 3 - 1, dx = t % 3 - 1;
+        if (EPI == CONV_DGELU) {
+          dy = -dy;
+          dx = -dx;
         }
-      } else if (EPI == CONV_LINEAR) {
-        float* o = static_cast<float*>(out0) + p * CO;
+        const uint32_t at = a0 + (uint32_t)(((r + 1 + dy) * kRowPitch + 1 + dx) * 16);
 #pragma unroll
-        for (int c4 = 0; c4 < CO / 4; c4++) {
-          float4 v;
-          v.x = acc[c4 * 4 + 0] + bias[c4 * 4 + 0];
-          v.y = acc[c4 * 4 + 1] + bias[c4 * 4 + 1];
-          v.z = acc[c4 * 4 + 2] + bias[c4 * 4 + 2];
-          v.w = acc[c4 * 4 + 3] + bias[c4 * 4 + 3];
-          *reinterpret_cast<float4*>(o + c4 * 4) = v;
-        }
-      } else {
-        const __nv_bfloat16* zp = zprev + p * CO;
-        __nv_bfloat16* d = static_cast<__nv_bfloat16*>(out0) + p * CO;
-#pragma unroll
-        for (int c8 = 0; c8 < CO / 8; c8++) {
-          const uint4 zv = *reinterpret_cast<const uint4*>(zp + c8 * 8);
-          const __nv_bfloat16* zs = reinterpret_cast<const __nv_bfloat16*>(&zv);
-          __align__(16) __nv_bfloat16 db[8];
-#pragma unroll
-          for (int q = 0; q < 8; q++) db[q] = __float2bfloat16_rn(acc[c8 * 8 + q] * gelu_grad(__bfloat162float(zs[q])));
-          *reinterpret_cast<uint4*>(d + c8 * 8) = *reinterpret_cast<const uint4*>(db);
+        for (int kc = 0; kc < CG / 16; kc++) {
+          const uint64_t da = umma::desc(at + kc * 2 * S::kLboA, S::kLboA, 128);
+          const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * S::kLboB, S::kLboB, 128);
+          umma::mma_bf16(tmem + (uint32_t)(r * CO), da, db, idesc, (t | kc) ? 1u : 0u);
         }
       }
+    umma::commit(bar);
+  }
+  __syncwarp();
+  const bool ok = wait_mma(bar, 0, err);
+  umma::fence_after_sync();
+  if (ok) {
+    const int q = warp & 3;  // the warp's tensor-memory lane quarter: pixels 32 q .. 32 q + 31
+    for (int r = warp >> 2; r < kRows; r += kRowThreads / 128) {
+      float acc[CO];
+#pragma unroll
+      for (int c8 = 0; c8 < CO / 8; c8++)
+        umma::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(r * CO + c8 * 8), acc + c8 * 8);
+      const long long p = (b * h + y0 + r) * (long long)w + x0 + q * 32 + lane;
+      epilogue<CO, EPI>(acc, p, bias, zprev, out0, out1);
     }
   }
   umma::fence_before_sync();
@@ -372,9 +510,18 @@ cudaError_t set_smem(K kernel, uint32_t bytes) {
 
 int g_sms = 0;  // SM count of the device the kernels were prepared on
 
+// Images whose width is a multiple of 128 and height a multiple of kRows take
+// the row kernel (the tile is staged once; taps are descriptor shifts),
+// others the gather kernel.
 template <int CG, int CO, int EPI>
 cudaError_t launch_conv(const __nv_bfloat16* x, int batch, int h, int w, const __nv_bfloat16* wt, const float* bias,
                         const __nv_bfloat16* zprev, void* out0, void* out1, int* err, cudaStream_t s) {
+  if (w % kRowPix == 0 && h % kRows == 0) {
+    const long long ctas = (long long)batch * (h / kRows) * (w / kRowPix);
+    conv3x3_rows_kernel<CG, CO, EPI><<<(unsigned)ctas, kRowThreads, RowSmem<CG, CO>::kLaunchBytes, s>>>(
+        x, wt, bias, zprev, batch, h, w, out0, out1, err);
+    return cudaGetLastError();
+  }
   using S = ConvSmem<CG, CO>;
   auto k = conv3x3_kernel<CG, CO, EPI>;
   const long long P = (long long)batch * h * w;
@@ -416,6 +563,10 @@ cudaError_t conv_prepare() {
   if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 16, CONV_LINEAR>, ConvSmem<32, 16>::kBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_kernel<16, 32, CONV_DGELU>, ConvSmem<16, 32>::kBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 32, CONV_DGELU>, ConvSmem<32, 32>::kBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 32, CONV_GELU>, RowSmem<32, 32>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 16, CONV_LINEAR>, RowSmem<32, 16>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<16, 32, CONV_DGELU>, RowSmem<16, 32>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 32, CONV_DGELU>, RowSmem<32, 32>::kLaunchBytes);
   if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 32>, WgradSmem<32, 32>::kBytes);
   if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 16>, WgradSmem<32, 16>::kBytes);
   return e;

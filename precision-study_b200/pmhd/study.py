@@ -13,6 +13,13 @@
         of every other run against fp64 per conserved variable and per .dat
         primitive column.  The exact-vs-FMA fp64 pair is the rounding noise
         floor the mixed result is measured against.
+
+    python -m pmhd.study conv --batch 8 --n 512 [--reps 20]
+        Times one layer of the learned correction's network (pmhd_conv3x3,
+        GELU, 32 -> 32 channels, bf16 NHWC images, tcgen05) on seeded data:
+        microseconds per call (CUDA events around each call, which includes
+        the call's own stream synchronisation), its FLOP rate and the
+        algorithmic HBM bytes (input read once, z and gelu(z) written).
 """
 import argparse
 import json
@@ -98,6 +105,50 @@ def run_study(n, t_end, problem_name, ny=None, runs_wanted=None):
     return {"problem": problem_name, "nx": n, "ny": ny, "t_end": t_end, "runs": runs}
 
 
+def conv_bench(batch, n, reps=20, seed=7):
+    """One GELU 3x3 layer (32 -> 32) over batch x n x n periodic images."""
+    import ctypes
+
+    import torch
+
+    from . import CONV_GELU, OK, load, strerror
+
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    cin = cout = 32
+    x = torch.randn((batch, n, n, cin), generator=g).to(torch.bfloat16).cuda()
+    w = (torch.randn((cout, 9, cin), generator=g) * 0.1).to(torch.bfloat16).cuda()
+    b = torch.zeros((cout,), dtype=torch.float32, device="cuda")
+    z = torch.empty((batch, n, n, cout), dtype=torch.bfloat16, device="cuda")
+    a = torch.empty_like(z)
+    L = load()
+
+    def call():
+        rc = L.pmhd_conv3x3(CONV_GELU, x.data_ptr(), batch, n, n, cin, w.data_ptr(),
+                            ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_float)), cout, None, z.data_ptr(),
+                            a.data_ptr(), None)
+        if rc != OK:
+            raise RuntimeError(strerror(rc))
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        call()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e3)
+    us = float(np.median(times))
+    pixels = batch * n * n
+    flops = 2.0 * 9 * cin * cout * pixels
+    nbytes = pixels * (cin + 2 * cout) * 2
+    return {"layer": "3x3 conv 32->32 + GELU, bf16 in/out, fp32 accumulation", "batch": batch, "n": n,
+            "us_per_call_median": us, "tflops": flops / (us * 1e-6) / 1e12, "hbm_gbs": nbytes / (us * 1e-6) / 1e9,
+            "flop_per_call": flops, "algorithmic_bytes_per_call": nbytes, "reps": reps}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m pmhd.study")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -110,9 +161,15 @@ def main(argv=None):
     r.add_argument("--t-end", type=float, default=0.5)
     r.add_argument("--problem", choices=["ot", "kh_reflect"], default="ot")
     r.add_argument("--runs", default=None, help="comma list of fp64_exact, fp32, mixed (fp64 always runs)")
+    v = sub.add_parser("conv")
+    v.add_argument("--batch", type=int, default=8)
+    v.add_argument("--n", type=int, default=512)
+    v.add_argument("--reps", type=int, default=20)
     args = ap.parse_args(argv)
     if args.cmd == "compare":
         compare_dat(args.a, args.b)
+    elif args.cmd == "conv":
+        print(json.dumps(conv_bench(args.batch, args.n, args.reps)))
     else:
         wanted = None if args.runs is None else set(args.runs.split(","))
         print(json.dumps(run_study(args.n, args.t_end, args.problem, args.ny, wanted)))

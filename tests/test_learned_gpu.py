@@ -86,7 +86,9 @@ def _bf(a):
     return C.bf16_round(a).astype(np.float64)
 
 
-SHAPES = [(1, 8, 16), (2, 9, 20), (1, 64, 64), (3, 17, 33)]
+# The last two shapes take the row kernel (width a multiple of 128, height
+# of 8), the others the gather kernel.
+SHAPES = [(1, 8, 16), (2, 9, 20), (1, 64, 64), (3, 17, 33), (1, 8, 128), (2, 16, 256)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -113,7 +115,7 @@ def test_forward_linear_exact_on_integers(pmhd_lib, shape):
 
 
 @pytest.mark.parametrize("cin", [16, 32])
-@pytest.mark.parametrize("shape", SHAPES[:3])
+@pytest.mark.parametrize("shape", SHAPES[:3] + SHAPES[4:])
 def test_backward_input_exact_on_integers(pmhd_lib, shape, cin):
     """x = the layer's output gradient (cin channels), W the layer weight
     [cin][9][32]; the kernel takes W transposed to [32][9][cin]."""
