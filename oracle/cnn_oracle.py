@@ -12,12 +12,13 @@ finite differences in float64 (tests/test_learned_oracle.py).
 Conventions (the kernels' own): images are NHWC arrays [batch, h, w, c],
 periodic in y and x; weights W[c_out, 9, c_in] with tap t = (dy+1)*3 +
 (dx+1) and out(y, x) = sum_t W[:, t, :] @ x(y+dy, x+dx) + b; GELU is the
-erf form 0.5 z (1 + erf(z / sqrt 2)) = 0.5 z erfc(-z / sqrt 2).
+tanh form 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), written as
+z / (1 + exp(-2 sqrt(2/pi) (z + 0.044715 z^3))) (the same function; no
+cancellation in the left tail).
 """
 import math
 
 import numpy as np
-from scipy.special import erfc
 
 TAPS = [(t // 3 - 1, t % 3 - 1) for t in range(9)]
 
@@ -39,13 +40,26 @@ def from_bf16_bits(u):
     return (np.asarray(u, dtype=np.uint32) << 16).view(np.float32)
 
 
+# y2 = 2 sqrt(2/pi) (z + 0.044715 z^3) = z (GELU_A + GELU_B z^2)
+GELU_A = 2.0 * math.sqrt(2.0 / math.pi)
+GELU_B = GELU_A * 0.044715
+
+
+def _gelu_sigmoid(z):
+    z = np.asarray(z, dtype=np.float64)
+    y2 = z * (GELU_A + GELU_B * z * z)
+    with np.errstate(over="ignore"):
+        return 1.0 / (1.0 + np.exp(-y2))
+
+
 def gelu(z):
-    # 1 + erf(u) = erfc(-u): no cancellation in the left tail.
-    return 0.5 * z * erfc(-z / math.sqrt(2.0))
+    return np.asarray(z, dtype=np.float64) * _gelu_sigmoid(z)
 
 
 def gelu_grad(z):
-    return 0.5 * erfc(-z / math.sqrt(2.0)) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    z = np.asarray(z, dtype=np.float64)
+    s = _gelu_sigmoid(z)
+    return s + z * s * (1.0 - s) * (GELU_A + 3.0 * GELU_B * z * z)
 
 
 def shift(x, dy, dx):

@@ -31,11 +31,31 @@ namespace {
 
 constexpr uint32_t kWaitPolls = 1u << 22;
 
-// GELU in the erf form, written with erfc (1 + erf(u) = erfc(-u)) so the
-// left tail keeps its relative accuracy instead of cancelling to zero.
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * erfcf(-z * 0.70710678118654752f); }
+// GELU in the tanh form, 0.5 z (1 + tanh(y)) with y = sqrt(2/pi) (z + 0.044715
+// z^3), written as z s with s = 1 / (1 + exp(-2 y)): one hardware exp2 and
+// one reciprocal, and the left tail keeps its relative accuracy (s is never
+// formed as a difference).  Its derivative: s + z s (1 - s) dy2/dz.
+constexpr float kGeluA = 1.5957691216057308f;     // 2 sqrt(2 / pi)
+constexpr float kGeluB = 0.071354816272737f;      // 2 sqrt(2 / pi) 0.044715
+constexpr float kLog2e = 1.4426950408889634f;
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float gelu_sigmoid(float z) {
+  const float y2 = z * (kGeluA + kGeluB * z * z);
+  return rcp_approx(1.0f + ex2_approx(-y2 * kLog2e));
+}
+__device__ __forceinline__ float gelu(float z) { return z * gelu_sigmoid(z); }
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * erfcf(-z * 0.70710678118654752f) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float s = gelu_sigmoid(z);
+  return s + z * s * (1.0f - s) * (kGeluA + 3.0f * kGeluB * z * z);
 }
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -69,7 +89,8 @@ __device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t parity, int* er
   return ok;
 }
 
-// Epilogue of one output pixel p from its CO fp32 accumulators.
+// Epilogue of one output pixel p from its CO fp32 accumulators; `bias` is
+// the CTA's 16-byte-aligned shared copy (unused by CONV_DGELU).
 template <int CO, int EPI>
 __device__ __forceinline__ void epilogue(const float (&acc)[CO], long long p, const float* __restrict__ bias,
                                          const __nv_bfloat16* __restrict__ zprev, void* __restrict__ out0,
@@ -79,12 +100,16 @@ __device__ __forceinline__ void epilogue(const float (&acc)[CO], long long p, co
     __nv_bfloat16* a = static_cast<__nv_bfloat16*>(out1) + p * CO;
 #pragma unroll
     for (int c8 = 0; c8 < CO / 8; c8++) {
-      __align__(16) __nv_bfloat16 zb[8], ab[8];
+      __align__(16) __nv_bfloat162 zb[4], ab[4];
+      const float4 b0 = reinterpret_cast<const float4*>(bias)[c8 * 2];
+      const float4 b1 = reinterpret_cast<const float4*>(bias)[c8 * 2 + 1];
+      const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const float zz = acc[c8 * 8 + q] + bias[c8 * 8 + q];
-        zb[q] = __float2bfloat16_rn(zz);
-        ab[q] = __float2bfloat16_rn(gelu(zz));
+      for (int q = 0; q < 4; q++) {
+        const float z0 = acc[c8 * 8 + 2 * q] + bb[2 * q];
+        const float z1 = acc[c8 * 8 + 2 * q + 1] + bb[2 * q + 1];
+        zb[q] = __floats2bfloat162_rn(z0, z1);
+        ab[q] = __floats2bfloat162_rn(gelu(z0), gelu(z1));
       }
       *reinterpret_cast<uint4*>(z + c8 * 8) = *reinterpret_cast<const uint4*>(zb);
       *reinterpret_cast<uint4*>(a + c8 * 8) = *reinterpret_cast<const uint4*>(ab);
@@ -93,11 +118,12 @@ __device__ __forceinline__ void epilogue(const float (&acc)[CO], long long p, co
     float* o = static_cast<float*>(out0) + p * CO;
 #pragma unroll
     for (int c4 = 0; c4 < CO / 4; c4++) {
+      const float4 b = reinterpret_cast<const float4*>(bias)[c4];
       float4 v;
-      v.x = acc[c4 * 4 + 0] + bias[c4 * 4 + 0];
-      v.y = acc[c4 * 4 + 1] + bias[c4 * 4 + 1];
-      v.z = acc[c4 * 4 + 2] + bias[c4 * 4 + 2];
-      v.w = acc[c4 * 4 + 3] + bias[c4 * 4 + 3];
+      v.x = acc[c4 * 4 + 0] + b.x;
+      v.y = acc[c4 * 4 + 1] + b.y;
+      v.z = acc[c4 * 4 + 2] + b.z;
+      v.w = acc[c4 * 4 + 3] + b.w;
       *reinterpret_cast<float4*>(o + c4 * 4) = v;
     }
   } else {
@@ -145,9 +171,11 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
   unsigned char* sB = smem + S::kOffB;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
+  __shared__ __align__(16) float sbias[CO];
   const int tid = threadIdx.x, warp = tid >> 5;
   const long long P = (long long)batch * h * w;
   const long long p0 = (long long)blockIdx.x * 128;
+  if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
 
   if (warp == 0) {
     umma::tmem_alloc(tslot, kCols);
@@ -211,7 +239,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
 #pragma unroll
     for (int c8 = 0; c8 < CO / 8; c8++) umma::ld8(tmem + ((uint32_t)(warp * 32) << 16) + c8 * 8, acc + c8 * 8);
     const long long p = p0 + tid;
-    if (p < P) epilogue<CO, EPI>(acc, p, bias, zprev, out0, out1);
+    if (p < P) epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -268,7 +296,9 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   unsigned char* sB = smem + S::kOffB;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
+  __shared__ __align__(16) float sbias[CO];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
   const int segs = w / kRowPix, rblocks = h / kRows;
   const int seg = (int)(blockIdx.x % segs);
   const int rb = (int)((blockIdx.x / segs) % rblocks);
@@ -292,15 +322,19 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   }
   // A operand: input rows y0 - 1 .. y0 + kRows, pixels x0 - 1 .. x0 + 128
   // (periodic), one 16-byte channel group per item; consecutive items are
-  // consecutive 16-byte words of the NHWC input.
+  // consecutive 16-byte words of the NHWC input.  Asynchronous 16-byte
+  // copies: all of a thread's items are in flight before it waits.
   for (int c = tid; c < (kRows + 2) * kRowPitch * (CG / 8); c += kRowThreads) {
     const int g = c % (CG / 8);
     const int px = (c / (CG / 8)) % kRowPitch;
     const int r = c / ((CG / 8) * kRowPitch);
     const int yy = wrap(y0 - 1 + r, h), xx = wrap(x0 - 1 + px, w);
-    const uint4 v = *reinterpret_cast<const uint4*>(x + ((b * h + yy) * (long long)w + xx) * CG + g * 8);
-    *reinterpret_cast<uint4*>(sA + g * S::kLboA + (r * kRowPitch + px) * 16) = v;
+    const uint32_t dst = smem_u32(sA + g * S::kLboA + (r * kRowPitch + px) * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                 "l"(x + ((b * h + yy) * (long long)w + xx) * CG + g * 8)
+                 : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   fence_proxy_async_smem();
   umma::fence_before_sync();
   __syncthreads();
@@ -339,7 +373,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
       for (int c8 = 0; c8 < CO / 8; c8++)
         umma::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(r * CO + c8 * 8), acc + c8 * 8);
       const long long p = (b * h + y0 + r) * (long long)w + x0 + q * 32 + lane;
-      epilogue<CO, EPI>(acc, p, bias, zprev, out0, out1);
+      epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
     }
   }
   umma::fence_before_sync();

@@ -691,7 +691,7 @@ int pmhd_learned_fine_run(pmhd_learned* L, int problem, const double* params, in
   return e == cudaSuccess ? PMHD_OK : PMHD_ERR_CUDA;
 }
 
-// File: "PMHDNET2", int32 n_params, Norm, n_params floats (four layers,
+// File: "PMHDNET3", int32 n_params, Norm, n_params floats (four layers,
 // physical-quantity outputs).
 int pmhd_learned_save(const pmhd_learned* L, const char* path) {
   if (!L || !path || !L->have_norm) return PMHD_ERR_ARG;
@@ -703,7 +703,7 @@ int pmhd_learned_save(const pmhd_learned* L, const char* path) {
   FILE* f = std::fopen(path, "wb");
   if (!f) return PMHD_ERR_IO;
   const int n = L->L.n_params;
-  bool ok = std::fwrite("PMHDNET2", 1, 8, f) == 8 && std::fwrite(&n, sizeof(int), 1, f) == 1 &&
+  bool ok = std::fwrite("PMHDNET3", 1, 8, f) == 8 && std::fwrite(&n, sizeof(int), 1, f) == 1 &&
             std::fwrite(&L->hnorm, sizeof(Norm), 1, f) == 1 &&
             std::fwrite(th.data(), sizeof(float), th.size(), f) == th.size();
   ok = (std::fclose(f) == 0) && ok;
@@ -718,7 +718,7 @@ int pmhd_learned_load(pmhd_learned* L, const char* path) {
   int n = 0;
   Norm nm;
   std::vector<float> th(L->L.n_params);
-  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PMHDNET2", 8) == 0 &&
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PMHDNET3", 8) == 0 &&
             std::fread(&n, sizeof(int), 1, f) == 1 && n == L->L.n_params &&
             std::fread(&nm, sizeof(Norm), 1, f) == 1 && std::fread(th.data(), sizeof(float), th.size(), f) == th.size();
   std::fclose(f);
