@@ -251,7 +251,9 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
 
 // Row kernel (forward / backward-data when the width is a multiple of 128
 // and the height of 8): a CTA of 8 warps computes kRows image rows x 128
-// pixels.  It stages the (kRows + 2) x 130 input pixels around them once
+// pixels (measured at batch 8 x 512^2: 8, 4 and 2 rows per CTA -- two to
+// four CTAs per SM -- run equally fast).  It stages the (kRows + 2) x 130
+// input pixels around them once
 // (periodic wrap), channel-group-interleaved: group g of 8 channels at
 // g * kLboA, then row, then pixel at 16 bytes -- the K-major no-swizzle
 // layout of an M = 128 operand whose rows are pixels.  The operand of tap
@@ -260,14 +262,14 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
 // the nine taps need no copies.  Accumulators: 128 lanes x CO columns per
 // row, kRows rows side by side in tensor memory.
 constexpr int kRowPix = 128;               // output pixels of a row segment (M)
-constexpr int kRows = 8;                   // output rows per CTA
+constexpr int kRows = 8;                   // output rows per CTA (default shape)
 constexpr int kRowPitch = kRowPix + 2;     // staged pixels per input row
 constexpr int kRowThreads = 256;
 
-template <int CG, int CO>
+template <int CG, int CO, int NR = kRows>
 struct RowSmem {
   static constexpr int K = 9 * CG;
-  static constexpr uint32_t kLboA = (uint32_t)(kRows + 2) * kRowPitch * 16u;  // channel-group stride of A
+  static constexpr uint32_t kLboA = (uint32_t)(NR + 2) * kRowPitch * 16u;  // channel-group stride of A
   static constexpr uint32_t kBytesA = (uint32_t)(CG / 8) * kLboA;
   static constexpr uint32_t kOffB = (kBytesA + 127u) & ~127u;
   static constexpr uint32_t kBytesB = (uint32_t)CO * K * 2u;
@@ -275,13 +277,15 @@ struct RowSmem {
   static constexpr uint32_t kOffBar = kOffB + kBytesB;
   static constexpr uint32_t kBytes = kOffBar + 16u;
   // Shared memory requested per CTA: at least enough that no more CTAs fit
-  // on an SM than its 512 tensor-memory columns hold (256 columns: two).
-  static constexpr uint32_t kTmemCols = umma::tmem_cols(kRows * CO);
-  static constexpr uint32_t kMinBytes = kTmemCols >= 256u ? 80u * 1024u : 0u;
+  // on an SM (228 KB) than its 512 tensor-memory columns hold; eight CTAs of
+  // 256 threads are the thread limit anyway.
+  static constexpr uint32_t kTmemCols = umma::tmem_cols(NR * CO);
+  static constexpr uint32_t kMaxCtas = 512u / kTmemCols;
+  static constexpr uint32_t kMinBytes = kMaxCtas >= 8u ? 0u : (228u * 1024u) / (kMaxCtas + 1u) + 1024u;
   static constexpr uint32_t kLaunchBytes = kBytes > kMinBytes ? kBytes : kMinBytes;
 };
 
-template <int CG, int CO, int EPI>
+template <int CG, int CO, int EPI, int NR = kRows>
 __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bfloat16* __restrict__ x,
                                                                    const __nv_bfloat16* __restrict__ wt,
                                                                    const float* __restrict__ bias,
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
                                                                    int batch, int h, int w,
                                                                    void* __restrict__ out0, void* __restrict__ out1,
                                                                    int* __restrict__ err) {
-  using S = RowSmem<CG, CO>;
+  using S = RowSmem<CG, CO, NR>;
   constexpr uint32_t kCols = S::kTmemCols;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* sA = smem;
@@ -299,11 +303,11 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   __shared__ __align__(16) float sbias[CO];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
-  const int segs = w / kRowPix, rblocks = h / kRows;
+  const int segs = w / kRowPix, rblocks = h / NR;
   const int seg = (int)(blockIdx.x % segs);
   const int rb = (int)((blockIdx.x / segs) % rblocks);
   const long long b = blockIdx.x / ((long long)segs * rblocks);
-  const int x0 = seg * kRowPix, y0 = rb * kRows;
+  const int x0 = seg * kRowPix, y0 = rb * NR;
   (void)batch;
 
   if (warp == 0) {
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   // (periodic), one 16-byte channel group per item; consecutive items are
   // consecutive 16-byte words of the NHWC input.  Asynchronous 16-byte
   // copies: all of a thread's items are in flight before it waits.
-  for (int c = tid; c < (kRows + 2) * kRowPitch * (CG / 8); c += kRowThreads) {
+  for (int c = tid; c < (NR + 2) * kRowPitch * (CG / 8); c += kRowThreads) {
     const int g = c % (CG / 8);
     const int px = (c / (CG / 8)) % kRowPitch;
     const int r = c / ((CG / 8) * kRowPitch);
@@ -344,7 +348,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
     constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
     const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
 #pragma unroll 1
-    for (int r = 0; r < kRows; r++)
+    for (int r = 0; r < NR; r++)
 #pragma unroll 1
       for (int t = 0; t < 9; t++) {
         int dy = t / 3 - 1, dx = t % 3 - 1;
@@ -367,7 +371,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   umma::fence_after_sync();
   if (ok) {
     const int q = warp & 3;  // the warp's tensor-memory lane quarter: pixels 32 q .. 32 q + 31
-    for (int r = warp >> 2; r < kRows; r += kRowThreads / 128) {
+    for (int r = warp >> 2; r < NR; r += kRowThreads / 128) {
       float acc[CO];
 #pragma unroll
       for (int c8 = 0; c8 < CO / 8; c8++)
