@@ -172,7 +172,7 @@ def test_exact_ot256_plain_method_matches_reference_output(pmhd_lib, prec, tmp_p
 
 
 def test_fma_fp64_full_ot192_within_1e12_of_the_reference_arithmetic(pmhd_lib):
-    """North-star bar for the FMA build: relative L2 <= 1e-12 per variable
+    """The accuracy bar of the FMA build: relative L2 <= 1e-12 per variable
     against the reference CPU fp64 result, on the reference's own FMA-effect
     comparison (Orszag-Tang 192^2 to t = 0.5; the reference measured 6.41e-13
     for its GPU FMA build, logs/mhd/gpu_backend_20260718/
