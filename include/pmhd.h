@@ -256,7 +256,8 @@ int pmhd_ensemble_destroy(pmhd_ensemble* e);
  * tap t = (dy+1)*3 + (dx+1), out(y,x) = sum_t W[t] x(y+dy, x+dx) + bias.
  * Enqueued on `stream` (a cudaStream_t, NULL = default) and synchronised
  * before returning; all pointers are device pointers, 16-byte aligned.
- *   PMHD_CONV_GELU:   out0 = z (bf16), out1 = gelu(z) (bf16), (c_in, c_out) = (32, 32)
+ *   PMHD_CONV_GELU:   out0 = z (bf16), out1 = gelu(z) (bf16), (c_in, c_out) = (32, 32);
+ *                     gelu is the tanh form z / (1 + exp(-2 sqrt(2/pi) (z + 0.044715 z^3)))
  *   PMHD_CONV_LINEAR: out0 = fp32 result, (32, 16)
  *   PMHD_CONV_DGELU:  backward to the input of a GELU layer: x = the
  *                     layer's output gradient (c_in = its outputs), weight =
