@@ -573,7 +573,8 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, ma
                                for k in ("rho", "mean", "all")}
             out[name] = rec
         if len(shrinks) > 1:
-            path = os.path.join(tempfile.mkdtemp(), "net.bin")
+            tmpdir = tempfile.TemporaryDirectory()
+            path = os.path.join(tmpdir.name, "net.bin")
             L.save(path)
             for sh in shrinks[1:]:
                 with pmhd.Learned(nx=n, ny=n, refine=refine, max_pairs=1, seed=seed, device=device,
@@ -587,6 +588,7 @@ def bench_learned(pmhd, n, device, refine=4, t_end=0.25, iters=1500, every=1, ma
                             out[name]["relL2_vs_fine"][key] = err(corr, fine)
                         except pmhd.PmhdError as exc:
                             out[name][key] = f"failed: {exc}"
+            tmpdir.cleanup()
     return out
 
 
