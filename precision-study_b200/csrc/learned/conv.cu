@@ -21,6 +21,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "learned/conv.h"
 #include "learned/umma.cuh"
 
@@ -388,6 +390,199 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   }
 }
 
+// Persistent, warp-specialised form of the row kernel: one CTA per SM
+// loops over the row tiles; four producer warps stage tile k + 1 (16-byte
+// asynchronous copies) while one thread issues tile k's MMAs and eight
+// warps drain tile k - 1 from tensor memory.  Two staging buffers and two
+// accumulator buffers; the hand-offs are mbarriers:
+//   full[b]   producers -> MMA      staging buffer b holds its tile
+//   empty[b]  MMA commit -> producers  the MMAs that read buffer b are done
+//   tfull[b]  MMA commit -> epilogue   accumulator buffer b is complete
+//   tempty[b] epilogue -> MMA          accumulator buffer b has been read
+// Every wait is bounded; on expiry the CTA records the error and leaves.
+constexpr int kPipeEpiWarps = 8, kPipeProdWarps = 4;
+constexpr int kPipeThreads = 32 * (kPipeEpiWarps + kPipeProdWarps + 1);
+
+template <int CG, int CO>
+struct PipeSmem {
+  using R = RowSmem<CG, CO>;
+  static constexpr uint32_t kStage = (R::kBytesA + 127u) & ~127u;  // one staging buffer (A operand)
+  static constexpr uint32_t kOffB = 2u * kStage;
+  static constexpr uint32_t kOffBar = (kOffB + R::kBytesB + 7u) & ~7u;
+  static constexpr uint32_t kBytes = kOffBar + 8u * 8u + 16u;
+  static constexpr uint32_t kColsBuf = umma::tmem_cols(kRows * CO);
+  static constexpr uint32_t kTmemCols = 2u * kColsBuf;
+  // At most 512 / kTmemCols CTAs per SM (see RowSmem).
+  static constexpr uint32_t kMaxCtas = 512u / kTmemCols;
+  static constexpr uint32_t kMinBytes = (228u * 1024u) / (kMaxCtas + 1u) + 1024u;
+  static constexpr uint32_t kLaunchBytes = kBytes > kMinBytes ? kBytes : kMinBytes;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait agreed by the whole warp.
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity) {
+  return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity, kWaitPolls));
+}
+
+template <int CG, int CO, int EPI>
+__global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                       const __nv_bfloat16* __restrict__ wt,
+                                                                       const float* __restrict__ bias,
+                                                                       const __nv_bfloat16* __restrict__ zprev,
+                                                                       int batch, int h, int w,
+                                                                       void* __restrict__ out0,
+                                                                       void* __restrict__ out1,
+                                                                       int* __restrict__ err) {
+  using R = RowSmem<CG, CO>;
+  using S = PipeSmem<CG, CO>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* sB = smem + S::kOffB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kOffBar);
+  uint64_t* empty = full + 2;
+  uint64_t* tfull = full + 4;
+  uint64_t* tempty = full + 6;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 8);
+  __shared__ __align__(16) float sbias[CO];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int segs = w / kRowPix, rblocks = h / kRows;
+  const long long ntiles = (long long)batch * rblocks * segs;
+
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, S::kTmemCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 2; b++) {
+      mbar_init(full + b, kPipeProdWarps * 32);
+      mbar_init(empty + b, 1);
+      mbar_init(tfull + b, 1);
+      mbar_init(tempty + b, kPipeEpiWarps * 32);
+    }
+    fence_barrier_init();
+  }
+  if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
+  for (int c = tid; c < CO * (R::K / 8); c += kPipeThreads) {
+    const int n = c / (R::K / 8), g = c - n * (R::K / 8);
+    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * R::K + g * 8);
+    *reinterpret_cast<uint4*>(sB + n * 16 + g * R::kLboB) = v;
+  }
+  fence_proxy_async_smem();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  bool ok = true;
+
+  if (warp >= kPipeEpiWarps && warp < kPipeEpiWarps + kPipeProdWarps) {
+    // Producers: stage tile k into buffer k % 2 once the MMAs of tile k - 2
+    // (the buffer's previous tile) are done.
+    const int pt = tid - kPipeEpiWarps * 32;
+    int k = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+      const int b = k & 1;
+      if (k >= 2 && !warp_wait(empty + b, (uint32_t)((k >> 1) - 1) & 1u)) {
+        ok = false;
+        break;
+      }
+      const int seg = (int)(tile % segs), rb = (int)((tile / segs) % rblocks);
+      const long long bb = tile / ((long long)segs * rblocks);
+      const int x0 = seg * kRowPix, y0 = rb * kRows;
+      unsigned char* sA = smem + b * S::kStage;
+      for (int c = pt; c < (kRows + 2) * kRowPitch * (CG / 8); c += kPipeProdWarps * 32) {
+        const int g = c % (CG / 8);
+        const int px = (c / (CG / 8)) % kRowPitch;
+        const int r = c / ((CG / 8) * kRowPitch);
+        const int yy = wrap(y0 - 1 + r, h), xx = wrap(x0 - 1 + px, w);
+        const uint32_t dst = smem_u32(sA + g * R::kLboA + (r * kRowPitch + px) * 16);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                     "l"(x + ((bb * h + yy) * (long long)w + xx) * CG + g * 8)
+                     : "memory");
+      }
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      fence_proxy_async_smem();
+      mbar_arrive(full + b);
+    }
+  } else if (warp == kPipeEpiWarps + kPipeProdWarps) {
+    // MMA issuer: tile k from buffer k % 2 into accumulator buffer k % 2
+    // once the epilogue has read that buffer's previous tile (k - 2).
+    int k = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+      const int b = k & 1;
+      if (!warp_wait(full + b, (uint32_t)(k >> 1) & 1u) ||
+          (k >= 2 && !warp_wait(tempty + b, (uint32_t)((k >> 1) - 1) & 1u))) {
+        ok = false;
+        break;
+      }
+      umma::fence_after_sync();
+      if (lane == 0) {
+        constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
+        const uint32_t a0 = smem_u32(smem + b * S::kStage), b0 = smem_u32(sB);
+        const uint32_t d0 = tmem + (uint32_t)b * S::kColsBuf;
+#pragma unroll 1
+        for (int r = 0; r < kRows; r++)
+#pragma unroll 1
+          for (int t = 0; t < 9; t++) {
+            int dy = t / 3 - 1, dx = t % 3 - 1;
+            if (EPI == CONV_DGELU) {
+              dy = -dy;
+              dx = -dx;
+            }
+            const uint32_t at = a0 + (uint32_t)(((r + 1 + dy) * kRowPitch + 1 + dx) * 16);
+#pragma unroll
+            for (int kc = 0; kc < CG / 16; kc++) {
+              const uint64_t da = umma::desc(at + kc * 2 * R::kLboA, R::kLboA, 128);
+              const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * R::kLboB, R::kLboB, 128);
+              umma::mma_bf16(d0 + (uint32_t)(r * CO), da, db, idesc, (t | kc) ? 1u : 0u);
+            }
+          }
+        umma::commit(tfull + b);
+        umma::commit(empty + b);
+      }
+      __syncwarp();
+    }
+    // The last two tiles' commits on empty[] have arrived before the CTA
+    // leaves (those phases are the newest of their barriers).
+    for (int kk = k - 2; ok && kk < k; kk++)
+      if (kk >= 0 && !warp_wait(empty + (kk & 1), (uint32_t)(kk >> 1) & 1u)) ok = false;
+  } else {
+    // Epilogue warps: tile k from accumulator buffer k % 2.
+    int k = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, k++) {
+      const int b = k & 1;
+      if (!warp_wait(tfull + b, (uint32_t)(k >> 1) & 1u)) {
+        ok = false;
+        break;
+      }
+      umma::fence_after_sync();
+      const int seg = (int)(tile % segs), rb = (int)((tile / segs) % rblocks);
+      const long long bb = tile / ((long long)segs * rblocks);
+      const int x0 = seg * kRowPix, y0 = rb * kRows;
+      const int q = warp & 3;  // tensor-memory lane quarter: pixels 32 q .. 32 q + 31
+      for (int r = warp >> 2; r < kRows; r += kPipeEpiWarps / 4) {
+        float acc[CO];
+#pragma unroll
+        for (int c8 = 0; c8 < CO / 8; c8++)
+          umma::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * S::kColsBuf + (uint32_t)(r * CO + c8 * 8),
+                    acc + c8 * 8);
+        const long long p = (bb * h + y0 + r) * (long long)w + x0 + q * 32 + lane;
+        epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
+      }
+      umma::fence_before_sync();
+      mbar_arrive(tempty + b);
+    }
+  }
+  if (!ok && lane == 0) atomicExch(err, PMHD_LEARNED_ERR_TIMEOUT);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, S::kTmemCols);
+  }
+}
+
 template <int CIN, int CO>
 struct WgradSmem {
   static constexpr int M = 9 * CIN;
@@ -549,12 +744,29 @@ cudaError_t set_smem(K kernel, uint32_t bytes) {
 int g_sms = 0;  // SM count of the device the kernels were prepared on
 
 // Images whose width is a multiple of 128 and height a multiple of kRows take
-// the row kernel (the tile is staged once; taps are descriptor shifts),
-// others the gather kernel.
+// the row kernels (the tile is staged once; taps are descriptor shifts) --
+// the persistent pipelined one from two row tiles per SM, else one CTA per
+// tile -- others the gather kernel.
 template <int CG, int CO, int EPI>
 cudaError_t launch_conv(const __nv_bfloat16* x, int batch, int h, int w, const __nv_bfloat16* wt, const float* bias,
                         const __nv_bfloat16* zprev, void* out0, void* out1, int* err, cudaStream_t s) {
   if (w % kRowPix == 0 && h % kRows == 0) {
+    const long long tiles = (long long)batch * (h / kRows) * (w / kRowPix);
+    const int sms = g_sms > 0 ? g_sms : 148;
+    // Test hook: PMHD_CONV_MAX_CTAS > 0 selects the persistent kernel on any
+    // row shape with at most that many CTAs, so small images still give each
+    // CTA several tiles (both buffers reused, barrier phases flipping).
+    const char* hook_env = getenv("PMHD_CONV_MAX_CTAS");
+    const long long hook = hook_env ? atoll(hook_env) : 0;
+    if (hook > 0 || tiles >= 2LL * sms) {
+      // Persistent, pipelined: pays off from two tiles per SM (8 x 512^2:
+      // 210 -> 182 us); one tile per CTA gains nothing from the pipeline.
+      long long grid = tiles < sms ? tiles : sms;
+      if (hook > 0 && grid > hook) grid = hook;
+      conv3x3_pipe_kernel<CG, CO, EPI><<<(unsigned)grid, kPipeThreads, PipeSmem<CG, CO>::kLaunchBytes, s>>>(
+          x, wt, bias, zprev, batch, h, w, out0, out1, err);
+      return cudaGetLastError();
+    }
     const long long ctas = (long long)batch * (h / kRows) * (w / kRowPix);
     conv3x3_rows_kernel<CG, CO, EPI><<<(unsigned)ctas, kRowThreads, RowSmem<CG, CO>::kLaunchBytes, s>>>(
         x, wt, bias, zprev, batch, h, w, out0, out1, err);
@@ -602,9 +814,13 @@ cudaError_t conv_prepare() {
   if (e == cudaSuccess) e = set_smem(conv3x3_kernel<16, 32, CONV_DGELU>, ConvSmem<16, 32>::kBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_kernel<32, 32, CONV_DGELU>, ConvSmem<32, 32>::kBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 32, CONV_GELU>, RowSmem<32, 32>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_pipe_kernel<32, 32, CONV_GELU>, PipeSmem<32, 32>::kLaunchBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 16, CONV_LINEAR>, RowSmem<32, 16>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_pipe_kernel<32, 16, CONV_LINEAR>, PipeSmem<32, 16>::kLaunchBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<16, 32, CONV_DGELU>, RowSmem<16, 32>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_pipe_kernel<16, 32, CONV_DGELU>, PipeSmem<16, 32>::kLaunchBytes);
   if (e == cudaSuccess) e = set_smem(conv3x3_rows_kernel<32, 32, CONV_DGELU>, RowSmem<32, 32>::kLaunchBytes);
+  if (e == cudaSuccess) e = set_smem(conv3x3_pipe_kernel<32, 32, CONV_DGELU>, PipeSmem<32, 32>::kLaunchBytes);
   if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 32>, WgradSmem<32, 32>::kBytes);
   if (e == cudaSuccess) e = set_smem(wgrad_kernel<32, 16>, WgradSmem<32, 16>::kBytes);
   return e;

@@ -132,6 +132,38 @@ def test_backward_input_exact_on_integers(pmhd_lib, shape, cin):
     np.testing.assert_array_equal(out == 0, ref == 0)
 
 
+@pytest.mark.parametrize("variant", ["gelu", "linear", "dgelu16", "dgelu32"])
+def test_pipelined_row_kernel_matches_the_per_tile_row_kernel(pmhd_lib, monkeypatch, variant):
+    """The persistent, pipelined row kernel (selected for large batches; here
+    forced by its test hook with 2 CTAs, so each CTA runs 8 tiles through
+    both staging and accumulator buffers) gives the per-tile row kernel's
+    results bit for bit (same MMA sequence per row), and both equal the
+    oracle on integer data."""
+    rng = np.random.default_rng(15)
+    shape = (4, 16, 256)
+    if variant == "gelu":
+        x, W, b, cout, zp, mode = _ints(rng, shape + (32,)), _ints(rng, (32, 9, 32), 0.2), \
+            rng.integers(-3, 4, 32).astype(np.float64), 32, None, pmhd_lib.CONV_GELU
+    elif variant == "linear":
+        x, W, b, cout, zp, mode = _ints(rng, shape + (32,)), _ints(rng, (16, 9, 32)), \
+            rng.integers(-3, 4, 16).astype(np.float64), 16, None, pmhd_lib.CONV_LINEAR
+    else:
+        cin = 16 if variant == "dgelu16" else 32
+        x = _ints(rng, shape + (cin,))
+        W = np.ascontiguousarray(_ints(rng, (cin, 9, 32), 0.3).transpose(2, 1, 0))
+        b, cout, mode = None, 32, pmhd_lib.CONV_DGELU
+        zp = _bf(rng.normal(0, 1.0, shape + (32,)))
+    monkeypatch.delenv("PMHD_CONV_MAX_CTAS", raising=False)
+    o0, o1 = _conv(pmhd_lib, mode, x, W, b, cout, zprev=zp)
+    monkeypatch.setenv("PMHD_CONV_MAX_CTAS", "2")
+    p0, p1 = _conv(pmhd_lib, mode, x, W, b, cout, zprev=zp)
+    np.testing.assert_array_equal(p0, o0)
+    if o1 is not None:
+        np.testing.assert_array_equal(p1, o1)
+    if variant in ("gelu", "linear"):
+        np.testing.assert_array_equal(p0, C.conv3x3(x, W, b))
+
+
 @pytest.mark.parametrize("cout", [32, 16])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_weight_gradient_exact_on_integers(pmhd_lib, shape, cout):
