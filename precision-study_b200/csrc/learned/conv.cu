@@ -7,10 +7,12 @@
 // (dx+1): out(y, x) = sum_t W[t] x(y+dy, x+dx) (cross-correlation).
 //
 // Implicit GEMM.  Forward / backward-data: M = 128 output pixels x N = c_out
-// channels, K = 9 taps x c_in channels.  Row kernel (width a multiple of
-// 128, height of 8): the CTA stages its rows' input once, each tap's operand
+// channels, K = 9 taps x c_in channels.  Row kernels (width a multiple of
+// 128, height of 8): a row tile's input is staged once, each tap's operand
 // is a shifted descriptor into it, one thread issues 8 rows x 9 * c_in / 16
-// tcgen05.mma, eight warps run the epilogue.  Gather kernel (other shapes):
+// tcgen05.mma, eight warps run the epilogue -- one CTA per tile, or (from
+// two tiles per SM) a persistent CTA per SM whose producer, MMA and
+// epilogue warps pipeline the tiles.  Gather kernel (other shapes):
 // one CTA per 128 pixels gathers the 9 shifted copies of its pixels' input
 // vectors (periodic wrap) into K-major tiles, one thread issues 9 * c_in / 16
 // tcgen05.mma, the four warps read the 128 x N accumulator back with
@@ -143,6 +145,19 @@ __device__ __forceinline__ void epilogue(const float (&acc)[CO], long long p, co
   }
 }
 
+// B operand: the weights [CO][9 CG], K-groups of 8 (16-byte vectors) at
+// kLboB = CO * 16; thread t of nt.
+template <int CG, int CO>
+__device__ __forceinline__ void stage_weights(unsigned char* sB, const __nv_bfloat16* __restrict__ wt, int t,
+                                              int nt) {
+  constexpr int K = 9 * CG;
+  for (int c = t; c < CO * (K / 8); c += nt) {
+    const int n = c / (K / 8), g = c - n * (K / 8);
+    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * K + g * 8);
+    *reinterpret_cast<uint4*>(sB + n * 16 + g * CO * 16) = v;
+  }
+}
+
 template <int CG, int CO>
 struct ConvSmem {
   static constexpr int K = 9 * CG;
@@ -187,12 +202,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
     mbar_init(bar, 1);
     fence_barrier_init();
   }
-  // B operand: weights, row n, K-groups of 8 (16-byte vectors).
-  for (int c = tid; c < CO * (S::K / 8); c += 128) {
-    const int n = c / (S::K / 8), g = c - n * (S::K / 8);
-    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * S::K + g * 8);
-    *reinterpret_cast<uint4*>(sB + n * 16 + g * S::kLboB) = v;
-  }
+  stage_weights<CG, CO>(sB, wt, tid, 128);
   // A operand: for each tap, the 128 pixels' shifted input vectors.
   for (int c = tid; c < 9 * 128 * (CG / 8); c += 128) {
     const int g = c % (CG / 8);
@@ -251,43 +261,118 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __nv_bfloat16* __res
   }
 }
 
-// Row kernel (forward / backward-data when the width is a multiple of 128
-// and the height of 8): a CTA of 8 warps computes kRows image rows x 128
-// pixels (measured at batch 8 x 512^2: 8, 4 and 2 rows per CTA -- two to
-// four CTAs per SM -- run equally fast).  It stages the (kRows + 2) x 130
-// input pixels around them once
-// (periodic wrap), channel-group-interleaved: group g of 8 channels at
-// g * kLboA, then row, then pixel at 16 bytes -- the K-major no-swizzle
-// layout of an M = 128 operand whose rows are pixels.  The operand of tap
-// (dy, dx) for output row r is then the same tile seen from pixel (1 + dx)
-// of staged row (r + 1 + dy): a shift of the descriptor's start address, so
-// the nine taps need no copies.  Accumulators: 128 lanes x CO columns per
-// row, kRows rows side by side in tensor memory.
 constexpr int kRowPix = 128;               // output pixels of a row segment (M)
-constexpr int kRows = 8;                   // output rows per CTA (default shape)
+constexpr int kRows = 8;                   // output rows per tile
 constexpr int kRowPitch = kRowPix + 2;     // staged pixels per input row
 constexpr int kRowThreads = 256;
+constexpr uint32_t kRowLboA = (uint32_t)(kRows + 2) * kRowPitch * 16u;  // channel-group stride of A
 
-template <int CG, int CO, int NR = kRows>
+template <int CG, int CO>
 struct RowSmem {
   static constexpr int K = 9 * CG;
-  static constexpr uint32_t kLboA = (uint32_t)(NR + 2) * kRowPitch * 16u;  // channel-group stride of A
-  static constexpr uint32_t kBytesA = (uint32_t)(CG / 8) * kLboA;
+  static constexpr uint32_t kBytesA = (uint32_t)(CG / 8) * kRowLboA;
   static constexpr uint32_t kOffB = (kBytesA + 127u) & ~127u;
   static constexpr uint32_t kBytesB = (uint32_t)CO * K * 2u;
-  static constexpr uint32_t kLboB = (uint32_t)CO * 16u;
   static constexpr uint32_t kOffBar = kOffB + kBytesB;
   static constexpr uint32_t kBytes = kOffBar + 16u;
   // Shared memory requested per CTA: at least enough that no more CTAs fit
   // on an SM (228 KB) than its 512 tensor-memory columns hold; eight CTAs of
   // 256 threads are the thread limit anyway.
-  static constexpr uint32_t kTmemCols = umma::tmem_cols(NR * CO);
+  static constexpr uint32_t kTmemCols = umma::tmem_cols(kRows * CO);
   static constexpr uint32_t kMaxCtas = 512u / kTmemCols;
   static constexpr uint32_t kMinBytes = kMaxCtas >= 8u ? 0u : (228u * 1024u) / (kMaxCtas + 1u) + 1024u;
   static constexpr uint32_t kLaunchBytes = kBytes > kMinBytes ? kBytes : kMinBytes;
 };
 
-template <int CG, int CO, int EPI, int NR = kRows>
+// A row tile: image bb, output rows y0 .. y0 + kRows - 1, pixels x0 .. x0 + 127.
+struct RowTile {
+  long long bb;
+  int y0, x0;
+};
+__device__ __forceinline__ RowTile row_tile(long long tile, int h, int w) {
+  const int segs = w / kRowPix, rblocks = h / kRows;
+  RowTile t;
+  t.x0 = (int)(tile % segs) * kRowPix;
+  t.y0 = (int)((tile / segs) % rblocks) * kRows;
+  t.bb = tile / ((long long)segs * rblocks);
+  return t;
+}
+
+// A operand of a row tile: input rows y0 - 1 .. y0 + kRows, pixels
+// x0 - 1 .. x0 + 128 (periodic), one 16-byte channel group per item
+// (consecutive items are consecutive 16-byte words of the NHWC input), by
+// asynchronous copies from thread t of nt; the caller waits for them.
+template <int CG>
+__device__ __forceinline__ void stage_row_tile(unsigned char* sA, const __nv_bfloat16* __restrict__ x,
+                                               const RowTile& rt, int h, int w, int t, int nt) {
+  for (int c = t; c < (kRows + 2) * kRowPitch * (CG / 8); c += nt) {
+    const int g = c % (CG / 8);
+    const int px = (c / (CG / 8)) % kRowPitch;
+    const int r = c / ((CG / 8) * kRowPitch);
+    const int yy = wrap(rt.y0 - 1 + r, h), xx = wrap(rt.x0 - 1 + px, w);
+    const uint32_t dst = smem_u32(sA + g * kRowLboA + (r * kRowPitch + px) * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                 "l"(x + ((rt.bb * h + yy) * (long long)w + xx) * CG + g * 8)
+                 : "memory");
+  }
+}
+
+// The row tile's MMAs, issued by one thread: for output row r and tap
+// (dy, dx) (mirrored for CONV_DGELU) the A operand is the staged tile seen
+// from pixel 1 + dx of staged row r + 1 + dy -- a shift of the descriptor's
+// start address; accumulators of row r at d0 + r * CO.
+template <int CG, int CO, int EPI>
+__device__ __forceinline__ void issue_row_mmas(uint32_t a0, uint32_t b0, uint32_t d0) {
+  constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
+  constexpr uint32_t kLboB = (uint32_t)CO * 16u;
+#pragma unroll 1
+  for (int r = 0; r < kRows; r++)
+#pragma unroll 1
+    for (int t = 0; t < 9; t++) {
+      int dy = t / 3 - 1, dx = t % 3 - 1;
+      if (EPI == CONV_DGELU) {
+        dy = -dy;
+        dx = -dx;
+      }
+      const uint32_t at = a0 + (uint32_t)(((r + 1 + dy) * kRowPitch + 1 + dx) * 16);
+#pragma unroll
+      for (int kc = 0; kc < CG / 16; kc++) {
+        const uint64_t da = umma::desc(at + kc * 2 * kRowLboA, kRowLboA, 128);
+        const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * kLboB, kLboB, 128);
+        umma::mma_bf16(d0 + (uint32_t)(r * CO), da, db, idesc, (t | kc) ? 1u : 0u);
+      }
+    }
+}
+
+// Reads a row tile's accumulators back (tensor-memory columns from tbase)
+// and runs the epilogue: warp `warp` of `nwarps` owns lane quarter warp % 4
+// (pixels 32 q .. 32 q + 31) of rows warp / 4, warp / 4 + nwarps / 4, ...
+template <int CO, int EPI>
+__device__ __forceinline__ void drain_row_tile(uint32_t tbase, int warp, int lane, int nwarps, const RowTile& rt,
+                                               int h, int w, const float* __restrict__ sbias,
+                                               const __nv_bfloat16* __restrict__ zprev, void* __restrict__ out0,
+                                               void* __restrict__ out1) {
+  const int q = warp & 3;
+  for (int r = warp >> 2; r < kRows; r += nwarps / 4) {
+    float acc[CO];
+#pragma unroll
+    for (int c8 = 0; c8 < CO / 8; c8++)
+      umma::ld8(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(r * CO + c8 * 8), acc + c8 * 8);
+    const long long p = (rt.bb * h + rt.y0 + r) * (long long)w + rt.x0 + q * 32 + lane;
+    epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
+  }
+}
+
+// Row kernel (forward / backward-data when the width is a multiple of 128
+// and the height of 8), one CTA of 8 warps per row tile of kRows image rows
+// x 128 pixels.  It stages the (kRows + 2) x 130 input pixels around them
+// once (periodic wrap), channel-group-interleaved: group g of 8 channels at
+// g * kRowLboA, then row, then pixel at 16 bytes -- the K-major no-swizzle
+// layout of an M = 128 operand whose rows are pixels, so the nine taps need
+// no copies (issue_row_mmas).  Accumulators: 128 lanes x CO columns per row,
+// kRows rows side by side in tensor memory.  (Measured at batch 8 x 512^2:
+// 8, 4 and 2 rows per CTA -- two to four CTAs per SM -- run equally fast.)
+template <int CG, int CO, int EPI>
 __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bfloat16* __restrict__ x,
                                                                    const __nv_bfloat16* __restrict__ wt,
                                                                    const float* __restrict__ bias,
@@ -295,7 +380,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
                                                                    int batch, int h, int w,
                                                                    void* __restrict__ out0, void* __restrict__ out1,
                                                                    int* __restrict__ err) {
-  using S = RowSmem<CG, CO, NR>;
+  using S = RowSmem<CG, CO>;
   constexpr uint32_t kCols = S::kTmemCols;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* sA = smem;
@@ -304,12 +389,7 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::kOffBar + 8);
   __shared__ __align__(16) float sbias[CO];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
-  const int segs = w / kRowPix, rblocks = h / NR;
-  const int seg = (int)(blockIdx.x % segs);
-  const int rb = (int)((blockIdx.x / segs) % rblocks);
-  const long long b = blockIdx.x / ((long long)segs * rblocks);
-  const int x0 = seg * kRowPix, y0 = rb * NR;
+  const RowTile rt = row_tile(blockIdx.x, h, w);
   (void)batch;
 
   if (warp == 0) {
@@ -320,26 +400,9 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
     mbar_init(bar, 1);
     fence_barrier_init();
   }
-  // B operand: weights, row n, K-groups of 8 (16-byte vectors).
-  for (int c = tid; c < CO * (S::K / 8); c += kRowThreads) {
-    const int n = c / (S::K / 8), g = c - n * (S::K / 8);
-    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * S::K + g * 8);
-    *reinterpret_cast<uint4*>(sB + n * 16 + g * S::kLboB) = v;
-  }
-  // A operand: input rows y0 - 1 .. y0 + kRows, pixels x0 - 1 .. x0 + 128
-  // (periodic), one 16-byte channel group per item; consecutive items are
-  // consecutive 16-byte words of the NHWC input.  Asynchronous 16-byte
-  // copies: all of a thread's items are in flight before it waits.
-  for (int c = tid; c < (NR + 2) * kRowPitch * (CG / 8); c += kRowThreads) {
-    const int g = c % (CG / 8);
-    const int px = (c / (CG / 8)) % kRowPitch;
-    const int r = c / ((CG / 8) * kRowPitch);
-    const int yy = wrap(y0 - 1 + r, h), xx = wrap(x0 - 1 + px, w);
-    const uint32_t dst = smem_u32(sA + g * S::kLboA + (r * kRowPitch + px) * 16);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
-                 "l"(x + ((b * h + yy) * (long long)w + xx) * CG + g * 8)
-                 : "memory");
-  }
+  if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
+  stage_weights<CG, CO>(sB, wt, tid, kRowThreads);
+  stage_row_tile<CG>(sA, x, rt, h, w, tid, kRowThreads);
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   fence_proxy_async_smem();
   umma::fence_before_sync();
@@ -347,41 +410,13 @@ __global__ void __launch_bounds__(kRowThreads) conv3x3_rows_kernel(const __nv_bf
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
   if (tid == 0) {
-    constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
-    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll 1
-    for (int r = 0; r < NR; r++)
-#pragma unroll 1
-      for (int t = 0; t < 9; t++) {
-        int dy = t / 3 - 1, dx = t % 3 - 1;
-        if (EPI == CONV_DGELU) {
-          dy = -dy;
-          dx = -dx;
-        }
-        const uint32_t at = a0 + (uint32_t)(((r + 1 + dy) * kRowPitch + 1 + dx) * 16);
-#pragma unroll
-        for (int kc = 0; kc < CG / 16; kc++) {
-          const uint64_t da = umma::desc(at + kc * 2 * S::kLboA, S::kLboA, 128);
-          const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * S::kLboB, S::kLboB, 128);
-          umma::mma_bf16(tmem + (uint32_t)(r * CO), da, db, idesc, (t | kc) ? 1u : 0u);
-        }
-      }
+    issue_row_mmas<CG, CO, EPI>(smem_u32(sA), smem_u32(sB), tmem);
     umma::commit(bar);
   }
   __syncwarp();
   const bool ok = wait_mma(bar, 0, err);
   umma::fence_after_sync();
-  if (ok) {
-    const int q = warp & 3;  // the warp's tensor-memory lane quarter: pixels 32 q .. 32 q + 31
-    for (int r = warp >> 2; r < NR; r += kRowThreads / 128) {
-      float acc[CO];
-#pragma unroll
-      for (int c8 = 0; c8 < CO / 8; c8++)
-        umma::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(r * CO + c8 * 8), acc + c8 * 8);
-      const long long p = (b * h + y0 + r) * (long long)w + x0 + q * 32 + lane;
-      epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
-    }
-  }
+  if (ok) drain_row_tile<CO, EPI>(tmem, warp, lane, kRowThreads / 32, rt, h, w, sbias, zprev, out0, out1);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) {
@@ -436,7 +471,6 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
                                                                        void* __restrict__ out0,
                                                                        void* __restrict__ out1,
                                                                        int* __restrict__ err) {
-  using R = RowSmem<CG, CO>;
   using S = PipeSmem<CG, CO>;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* sB = smem + S::kOffB;
@@ -447,8 +481,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
   uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 8);
   __shared__ __align__(16) float sbias[CO];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int segs = w / kRowPix, rblocks = h / kRows;
-  const long long ntiles = (long long)batch * rblocks * segs;
+  const long long ntiles = (long long)batch * (h / kRows) * (w / kRowPix);
 
   if (warp == 0) {
     umma::tmem_alloc(tslot, S::kTmemCols);
@@ -464,11 +497,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
     fence_barrier_init();
   }
   if (tid < CO) sbias[tid] = EPI == CONV_DGELU ? 0.0f : bias[tid];
-  for (int c = tid; c < CO * (R::K / 8); c += kPipeThreads) {
-    const int n = c / (R::K / 8), g = c - n * (R::K / 8);
-    const uint4 v = *reinterpret_cast<const uint4*>(wt + (size_t)n * R::K + g * 8);
-    *reinterpret_cast<uint4*>(sB + n * 16 + g * R::kLboB) = v;
-  }
+  stage_weights<CG, CO>(sB, wt, tid, kPipeThreads);
   fence_proxy_async_smem();
   umma::fence_before_sync();
   __syncthreads();
@@ -487,20 +516,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
         ok = false;
         break;
       }
-      const int seg = (int)(tile % segs), rb = (int)((tile / segs) % rblocks);
-      const long long bb = tile / ((long long)segs * rblocks);
-      const int x0 = seg * kRowPix, y0 = rb * kRows;
-      unsigned char* sA = smem + b * S::kStage;
-      for (int c = pt; c < (kRows + 2) * kRowPitch * (CG / 8); c += kPipeProdWarps * 32) {
-        const int g = c % (CG / 8);
-        const int px = (c / (CG / 8)) % kRowPitch;
-        const int r = c / ((CG / 8) * kRowPitch);
-        const int yy = wrap(y0 - 1 + r, h), xx = wrap(x0 - 1 + px, w);
-        const uint32_t dst = smem_u32(sA + g * R::kLboA + (r * kRowPitch + px) * 16);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
-                     "l"(x + ((bb * h + yy) * (long long)w + xx) * CG + g * 8)
-                     : "memory");
-      }
+      stage_row_tile<CG>(smem + b * S::kStage, x, row_tile(tile, h, w), h, w, pt, kPipeProdWarps * 32);
       asm volatile("cp.async.wait_all;\n" ::: "memory");
       fence_proxy_async_smem();
       mbar_arrive(full + b);
@@ -518,26 +534,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
       }
       umma::fence_after_sync();
       if (lane == 0) {
-        constexpr uint32_t idesc = umma::idesc_bf16(128, CO, false, false);
-        const uint32_t a0 = smem_u32(smem + b * S::kStage), b0 = smem_u32(sB);
-        const uint32_t d0 = tmem + (uint32_t)b * S::kColsBuf;
-#pragma unroll 1
-        for (int r = 0; r < kRows; r++)
-#pragma unroll 1
-          for (int t = 0; t < 9; t++) {
-            int dy = t / 3 - 1, dx = t % 3 - 1;
-            if (EPI == CONV_DGELU) {
-              dy = -dy;
-              dx = -dx;
-            }
-            const uint32_t at = a0 + (uint32_t)(((r + 1 + dy) * kRowPitch + 1 + dx) * 16);
-#pragma unroll
-            for (int kc = 0; kc < CG / 16; kc++) {
-              const uint64_t da = umma::desc(at + kc * 2 * R::kLboA, R::kLboA, 128);
-              const uint64_t db = umma::desc(b0 + (t * (CG / 8) + kc * 2) * R::kLboB, R::kLboB, 128);
-              umma::mma_bf16(d0 + (uint32_t)(r * CO), da, db, idesc, (t | kc) ? 1u : 0u);
-            }
-          }
+        issue_row_mmas<CG, CO, EPI>(smem_u32(smem + b * S::kStage), smem_u32(sB),
+                                    tmem + (uint32_t)b * S::kColsBuf);
         umma::commit(tfull + b);
         umma::commit(empty + b);
       }
@@ -557,19 +555,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) conv3x3_pipe_kernel(const __n
         break;
       }
       umma::fence_after_sync();
-      const int seg = (int)(tile % segs), rb = (int)((tile / segs) % rblocks);
-      const long long bb = tile / ((long long)segs * rblocks);
-      const int x0 = seg * kRowPix, y0 = rb * kRows;
-      const int q = warp & 3;  // tensor-memory lane quarter: pixels 32 q .. 32 q + 31
-      for (int r = warp >> 2; r < kRows; r += kPipeEpiWarps / 4) {
-        float acc[CO];
-#pragma unroll
-        for (int c8 = 0; c8 < CO / 8; c8++)
-          umma::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * S::kColsBuf + (uint32_t)(r * CO + c8 * 8),
-                    acc + c8 * 8);
-        const long long p = (bb * h + y0 + r) * (long long)w + x0 + q * 32 + lane;
-        epilogue<CO, EPI>(acc, p, sbias, zprev, out0, out1);
-      }
+      drain_row_tile<CO, EPI>(tmem + (uint32_t)b * S::kColsBuf, warp, lane, kPipeEpiWarps, row_tile(tile, h, w), h,
+                              w, sbias, zprev, out0, out1);
       umma::fence_before_sync();
       mbar_arrive(tempty + b);
     }
