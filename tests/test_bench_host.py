@@ -147,3 +147,29 @@ def test_reference_gpu_zero_wall_gives_none(tmp_path, monkeypatch):
 def test_reference_gpu_absent_gives_none(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "REF_GPU", str(tmp_path / "missing_{}"))
     assert bench.run_reference_gpu(64) is None
+
+
+def test_reference_shock_bubble_time_is_parsed_from_its_stdout(tmp_path, monkeypatch):
+    """run_reference_euler_gpu reads the shock-bubble GPU program's own "Done.
+    Steps" and "Execution Time" lines (a fake program prints them; the median
+    of the timed runs after the warm-up is kept)."""
+    times = tmp_path / "times"
+    times.write_text("900.0\n330.0\n320.0\n340.0\n")
+    exe = tmp_path / "euler2d_gpu_fp64"
+    exe.write_text("#!/bin/sh\n"
+                   f"t=$(head -1 {times}); sed -i 1d {times}\n"
+                   "echo 'Done. Steps: 3459'\n"
+                   "echo \"Execution Time: $t ms (0.3 s)\"\n")
+    exe.chmod(0o755)
+    monkeypatch.setattr(bench, "REF_EULER_GPU", str(tmp_path / "euler2d_gpu_{}"))
+    r = bench.run_reference_euler_gpu("fp64")
+    assert r == {"ms": 330.0, "steps": 3459, "runs": 3, "warmup_runs": 1}
+    assert bench.run_reference_euler_gpu("fp32") is None  # no such program
+
+
+def test_reference_shock_bubble_failure_gives_none(tmp_path, monkeypatch):
+    exe = tmp_path / "euler2d_gpu_fp64"
+    exe.write_text("#!/bin/sh\necho 'CUDA Error at x:1 - no device'\nexit 1\n")
+    exe.chmod(0o755)
+    monkeypatch.setattr(bench, "REF_EULER_GPU", str(tmp_path / "euler2d_gpu_{}"))
+    assert bench.run_reference_euler_gpu("fp64") is None
