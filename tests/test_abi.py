@@ -133,3 +133,17 @@ def test_cli_without_device_exits_9(pmhd_lib):
     r = subprocess.run([CLI, "16", "16", "0.01"], capture_output=True, text=True)
     assert r.returncode == 9
     assert "Orszag-Tang" in r.stdout
+
+
+EULER_CLI = os.path.join(ROOT, "precision-study_b200", "bin", "euler2d_gpu")
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_euler_cli_without_device_exits_1(pmhd_lib):
+    """The shock-bubble drop-in prints the reference program's header lines
+    (euler2d_cuda.cu:290-296, :226-243, with its logged shock states) and,
+    without a B200, exits with EXIT_FAILURE as the reference's CUDA_CHECK."""
+    r = subprocess.run([EULER_CLI + "_fp32"], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "Grid: 500 x 197 (with 2 ghost -> 504 x 201)" in r.stdout
+    assert "Post-shock: rho=1.7755, p=159060.0, u=110.6272" in r.stdout

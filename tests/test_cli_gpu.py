@@ -122,3 +122,27 @@ def test_cli_lines_parse_like_the_reference_gpu_program(pmhd_lib, tmp_path):
     assert po["done"][0] == pr["done"][0]  # same step count
     assert po["evals"] == pr["evals"]
     assert os.path.basename(po["saved"][0]) == os.path.basename(pr["saved"][0])
+
+
+EULER_BIN = os.path.join(ROOT, "precision-study_b200", "bin", "euler2d_gpu")
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_euler_cli_writes_the_reference_program_data(pmhd_lib, tmp_path, prec):
+    """The shock-bubble drop-in (bin/euler2d_gpu_<prec>, replacing
+    src/euler/euler2d_cuda.cu): its progress and summary lines, and -- exact
+    kernels -- the data lines of gpu_shock_bubble.dat equal those of the
+    reference CPU program's cpu_shock_bubble.dat (tests/golden/euler_runs.json)."""
+    gold = next(r for r in json.load(open(os.path.join(HERE, "golden", "euler_runs.json")))["shock_bubble"]
+                if r["precision"] == prec)
+    env = dict(os.environ, OUTDIR=str(tmp_path), PMHD_EXACT="1")
+    r = subprocess.run([EULER_BIN + "_" + prec], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert int(re.search(r"Done\. Steps: (\d+)", r.stdout).group(1)) == gold["steps"]
+    assert re.search(r"Execution Time: [0-9.]+ ms \([0-9.]+ s\)", r.stdout)
+    assert len(re.findall(r"^Step \d+00: t = \S+$", r.stdout, re.M)) == gold["steps"] // 100
+    path = os.path.join(str(tmp_path), "gpu_shock_bubble.dat")
+    assert f"Saved {path}" in r.stdout
+    with open(path, "rb") as f:
+        assert f.readline().startswith(b"# Time = ")
+    assert md5_data(path) == gold["md5_data"]
