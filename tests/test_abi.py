@@ -147,3 +147,22 @@ def test_euler_cli_without_device_exits_1(pmhd_lib):
     assert r.returncode == 1
     assert "Grid: 500 x 197 (with 2 ghost -> 504 x 201)" in r.stdout
     assert "Post-shock: rho=1.7755, p=159060.0, u=110.6272" in r.stdout
+
+
+RIEMANN_CLI = os.path.join(ROOT, "precision-study_b200", "bin", "riemann2d_gpu")
+
+
+def test_riemann_cli_rejects_an_unknown_configuration(pmhd_lib):
+    r = subprocess.run([RIEMANN_CLI, "64", "5"], capture_output=True, text=True)
+    assert r.returncode == 1 and "config_id must be 3, 6, or 12" in r.stderr
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_riemann_cli_without_device_exits_1(pmhd_lib):
+    """The 2D Riemann drop-in prints the reference GPU program's header
+    (riemann2d_gpu.cu:344-350) and, without a B200, exits with EXIT_FAILURE
+    as the reference's CUDA_CHECK."""
+    r = subprocess.run([RIEMANN_CLI + "_fp32", "64", "3"], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "Config:    cfg3_4shocks  (id=3)" in r.stdout and "Precision: fp32" in r.stdout
+    assert "Grid:      64 x 64  dx=0.015625" in r.stdout and "T_end:     0.3" in r.stdout

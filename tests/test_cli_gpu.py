@@ -146,3 +146,26 @@ def test_euler_cli_writes_the_reference_program_data(pmhd_lib, tmp_path, prec):
     with open(path, "rb") as f:
         assert f.readline().startswith(b"# Time = ")
     assert md5_data(path) == gold["md5_data"]
+
+
+RIEMANN_BIN = os.path.join(ROOT, "precision-study_b200", "bin", "riemann2d_gpu")
+
+
+@pytest.mark.parametrize("n,config,prec", [(64, 3, "fp64"), (64, 6, "fp32"), (100, 3, "fp64")])
+def test_riemann_cli_writes_the_reference_program_output(pmhd_lib, tmp_path, n, config, prec):
+    """The 2D Riemann drop-in (bin/riemann2d_gpu_<prec> N config, replacing
+    src/euler/riemann2d_gpu.cu): step count, file name and -- exact kernels
+    -- the .dat file equal the reference CPU program's
+    (tests/golden/euler_runs.json)."""
+    gold = next(r for r in json.load(open(os.path.join(HERE, "golden", "euler_runs.json")))["runs2d"]
+                if (r["n"], r["config"], r["solver"], r["precision"]) == (n, config, "hllc", prec))
+    env = dict(os.environ, OUTDIR=str(tmp_path), PMHD_EXACT="1")
+    r = subprocess.run([RIEMANN_BIN + "_" + prec, str(n), str(config)], capture_output=True, text=True, env=env,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert re.search(r"Done\. Steps: (\d+)   Wall: \S+ s", r.stdout).group(1) == str(gold["steps"])
+    name = {3: "cfg3_4shocks", 6: "cfg6_4contacts", 12: "cfg12_2S2C"}[config]
+    path = os.path.join(str(tmp_path), f"riemann2d_{name}_hllc_{n}.dat")
+    assert f"Saved: {path}" in r.stdout
+    with open(path, "rb") as f:
+        assert hashlib.md5(f.read()).hexdigest() == gold["md5"]
