@@ -166,3 +166,19 @@ def test_riemann_cli_without_device_exits_1(pmhd_lib):
     assert r.returncode == 1
     assert "Config:    cfg3_4shocks  (id=3)" in r.stdout and "Precision: fp32" in r.stdout
     assert "Grid:      64 x 64  dx=0.015625" in r.stdout and "T_end:     0.3" in r.stdout
+
+
+RIEMANN1D_CLI = os.path.join(ROOT, "precision-study_b200", "bin", "riemann1d_gpu")
+
+
+def test_riemann1d_cli_rejects_an_unknown_test(pmhd_lib):
+    r = subprocess.run([RIEMANN1D_CLI, "200", "6"], capture_output=True, text=True)
+    assert r.returncode == 1 and "test_id must be 1-5" in r.stderr
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_riemann1d_cli_without_device_exits_1(pmhd_lib):
+    r = subprocess.run([RIEMANN1D_CLI + "_fp32", "200", "5", "hll"], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "Test:      Two_shocks  (id=5)" in r.stdout and "Solver:    HLL\n" in r.stdout
+    assert "N=200  dx=0.005" in r.stdout

@@ -169,3 +169,25 @@ def test_riemann_cli_writes_the_reference_program_output(pmhd_lib, tmp_path, n, 
     assert f"Saved: {path}" in r.stdout
     with open(path, "rb") as f:
         assert hashlib.md5(f.read()).hexdigest() == gold["md5"]
+
+
+RIEMANN1D_BIN = os.path.join(ROOT, "precision-study_b200", "bin", "riemann1d_gpu")
+
+
+@pytest.mark.parametrize("test,solver,prec", [(1, "hllc", "fp64"), (5, "hll", "fp64"), (3, "hllc", "fp32")])
+def test_riemann1d_cli_writes_the_reference_program_output(pmhd_lib, tmp_path, test, solver, prec):
+    """The 1D Riemann drop-in (bin/riemann1d_gpu_<prec> N test solver,
+    replacing src/euler/riemann1d_gpu.cu): step count, file name and -- exact
+    kernels -- the .dat file equal the reference CPU program's
+    (tests/golden/euler_runs.json)."""
+    gold = next(r for r in json.load(open(os.path.join(HERE, "golden", "euler_runs.json")))["runs1d"]
+                if (r["n"], r["test"], r["solver"], r["precision"]) == (200, test, solver, prec))
+    env = dict(os.environ, OUTDIR=str(tmp_path), PMHD_EXACT="1")
+    r = subprocess.run([RIEMANN1D_BIN + "_" + prec, "200", str(test), solver], capture_output=True, text=True,
+                       env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert int(re.search(r"Done\. Steps: (\d+)", r.stdout).group(1)) == gold["steps"]
+    path = os.path.join(str(tmp_path), f"toro{test}_{solver}_{prec}_200.dat")
+    assert f"Saved: {path}" in r.stdout
+    with open(path, "rb") as f:
+        assert hashlib.md5(f.read()).hexdigest() == gold["md5"]
