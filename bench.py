@@ -646,13 +646,18 @@ def main():
     ap.add_argument("--ref-n", type=int, default=4096, help="grid of one reference CPU sample")
     ap.add_argument("--ref-instances", type=int, default=64, help="max concurrent reference processes")
     ap.add_argument("--cpu-n", type=int, default=4096, help="grid of the 1-core cpu_baseline sample")
-    ap.add_argument("--ensemble", type=int, default=512, help="members of the ensemble line (0: skip)")
+    # The auxiliary lines (ensemble, learned correction, Euler, MUSCL-Hancock)
+    # are single-GPU measurements: on N > 1 ranks they default to off, so the
+    # scaling runs hold their GPUs only for the headline; a value given on the
+    # command line runs them on every N.
+    ap.add_argument("--ensemble", type=int, default=None, help="members of the ensemble line (0: skip; 512)")
     ap.add_argument("--ensemble-seed", type=int, default=20261203)
-    ap.add_argument("--learned", type=int, default=512, help="coarse grid of the learned-correction line (0: skip)")
+    ap.add_argument("--learned", type=int, default=None,
+                    help="coarse grid of the learned-correction line (0: skip; 512)")
     ap.add_argument("--learned-iters", type=int, default=1500, help="training iterations of the learned line")
-    ap.add_argument("--euler", type=int, default=4096, help="grid of the Euler-sibling line (0: skip)")
+    ap.add_argument("--euler", type=int, default=None, help="grid of the Euler-sibling line (0: skip; 4096)")
     ap.add_argument("--shock-bubble", type=int, default=1, help="whole shock-bubble runs in the Euler line (0: skip)")
-    ap.add_argument("--hancock", type=int, default=4096, help="grid of the MUSCL-Hancock line (0: skip)")
+    ap.add_argument("--hancock", type=int, default=None, help="grid of the MUSCL-Hancock line (0: skip; 4096)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -660,6 +665,9 @@ def main():
         return bench_reference(args)
 
     rank, world, local = dist_env()
+    for name, single_gpu_default in (("ensemble", 512), ("learned", 512), ("euler", 4096), ("hancock", 4096)):
+        if getattr(args, name) is None:
+            setattr(args, name, single_gpu_default if world == 1 else 0)
     dist = None
     if world > 1:
         import torch
